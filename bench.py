@@ -1,0 +1,364 @@
+#!/usr/bin/env python
+"""Update-and-measure throughput of SU(3) 32^4 Metropolis on B200.
+
+Workload (one step = one cycle of run_metropolis, Metropolis.hpp:204-218):
+one Metropolis sweep of SU(3) 32^4 (beta = 6, nHits = 10, proposals
+X = exp(i eps H), eps tuned to ~50% acceptance during 200 thermalisation
+sweeps from a cold start), then GaugePlaquette and WilsonLoop_temporal for all
+(L, T) in 1..8 (64 pairs, averaged over the 3 spatial directions).
+
+Metric: link updates/s (a link update = one link visited by the sweep, Nd*V per
+step), for the mixed form (FP32 links, FP64 reductions; `value`) and the plain
+FP64 form (`fp64`).  Inputs are synthetic (seeded cold start).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun (N > 1) every rank runs an independent replica (the path does
+not shard); `value` sums the ranks' link updates over the max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+L_DEFAULT = 32
+BETA, NHITS = 6.0, 10
+PAIRS = [(l, t) for l in range(1, 9) for t in range(1, 9)]
+METRIC = "Link updates/s (SU(3) 32^4), mixed vs FP64 form"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--L", type=int, default=L_DEFAULT)
+    ap.add_argument("--therm", type=int, default=200)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ distributed plumbing
+class Dist:
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+            torch.cuda.set_device(self.local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+            self.pg = dist
+
+    def set_device(self):
+        if self.world > 1:
+            from klft_b200 import _lib  # noqa: F401
+            import ctypes
+            ctypes.CDLL("libcudart.so.12", mode=ctypes.RTLD_GLOBAL).cudaSetDevice(self.local)
+
+    def barrier(self):
+        if self.pg:
+            import torch
+            self.pg.barrier(device_ids=[self.local])
+            torch.cuda.synchronize()
+
+    def max(self, x: float) -> float:
+        if not self.pg:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{self.local}")
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# ------------------------------------------------------------------ clocks
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, index: int = 0):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 3 + i and r[3 + i] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+# ------------------------------------------------------------------ our arm
+def thermalise(g, nsweeps: int, eps0: float = 0.25):
+    """Cold start -> nsweeps sweeps, tuning eps towards 50% acceptance (then frozen)."""
+    eps = eps0
+    done = 0
+    while done < nsweeps:
+        n = min(20, nsweeps - done)
+        acc = g.metropolis(BETA, 0.0, NHITS, n, proposal="exp", eps=eps)
+        a = float(acc[-1])
+        if a > 0.55:
+            eps *= 1.15
+        elif a < 0.45:
+            eps /= 1.15
+        done += n
+    return eps
+
+
+def time_cycles(g, eps, steps, warmup, clocks=None):
+    g.run_cycles(BETA, 0.0, NHITS, warmup, "exp", eps, True, PAIRS)
+    if clocks:
+        with clocks:
+            acc, plaq, w, ms = g.run_cycles(BETA, 0.0, NHITS, steps, "exp", eps, True, PAIRS)
+    else:
+        acc, plaq, w, ms = g.run_cycles(BETA, 0.0, NHITS, steps, "exp", eps, True, PAIRS)
+    return acc, plaq, w, ms
+
+
+def kernel_split(g, eps, reps=3):
+    """Device time of the sweep alone and of the measurement alone (ms per cycle)."""
+    _, _, _, ms_sweep = g.run_cycles(BETA, 0.0, NHITS, reps, "exp", eps, False, [])
+    _, _, _, ms_all = g.run_cycles(BETA, 0.0, NHITS, reps, "exp", eps, True, PAIRS)
+    return ms_sweep / reps, max(ms_all - ms_sweep, 0.0) / reps
+
+
+def e2e_public_api(g, eps, steps):
+    """Per step through the public API with host buffers: sweep, plaquette, W_temp."""
+    pairs = np.array(PAIRS, dtype=np.int32)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        g.metropolis(BETA, 0.0, NHITS, 1, proposal="exp", eps=eps)
+        g.plaquette()
+        g.wilson_loop_temporal(pairs)
+    dt = time.perf_counter() - t0
+    h2d = pairs.nbytes * 3  # the pair list goes up once per spatial direction
+    d2h = 8 + 8 + 8 * len(PAIRS) * 3
+    return dt, h2d, d2h
+
+
+def e2e_host_lattice(g, eps, steps):
+    """Per step: upload links from host, cycle, download links (users keeping configs on the host)."""
+    U = g.download()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        g.upload(U)
+        g.run_cycles(BETA, 0.0, NHITS, 1, "exp", eps, True, PAIRS)
+        U = g.download()
+    dt = time.perf_counter() - t0
+    return dt, U.nbytes, U.nbytes
+
+
+def peak(dtype):
+    import ctypes
+    from klft_b200._lib import lib
+    v = ctypes.c_double()
+    return v.value if lib().klft_peak_flops(dtype, ctypes.byref(v)) == 0 else None
+
+
+def measured_peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return {}
+
+
+def cpu_baseline_reference(L: int):
+    """klft's own code (oracle/_ref shim) on the host cores: one cycle of the same workload."""
+    from oracle.oracle import REF_SO, Lat, RefShim
+    if not os.path.exists(REF_SO):
+        from oracle.oracle import Oracle
+        return None
+    r = RefShim()
+    cores = r.set_threads(os.cpu_count() or 1)
+    lat = Lat(3, [L] * 4)
+    U = lat.field()
+    U[:, :, 0, 0] = U[:, :, 1, 1] = U[:, :, 2, 2] = 1.0
+    t0 = time.perf_counter()
+    r.cycles(lat, U, BETA, 0.1, NHITS, 1, 1234, PAIRS)
+    dt = time.perf_counter() - t0
+    return {"value": lat.V * 4 / dt, "unit": "link updates/s", "cores": cores, "kind": "reference",
+            "sample": f"1 cycle of SU(3) {L}^4 (sweep + plaquette + 64 temporal Wilson loops), klft's headers on "
+                      f"the project's Kokkos-API OpenMP shim, reference SU(3) proposal, {cores} threads, "
+                      f"{dt:.2f} s"}
+
+
+def run_ours(a, dist: Dist):
+    import klft_b200
+    dist.set_device()
+    L = [a.L] * 4
+    V = a.L ** 4
+    links_per_step = 4 * V
+    g = klft_b200.GaugeField(L, 3, "mixed", "cold", 1234 + dist.rank)
+    g.set_stream(1234, dist.rank)
+    eps = thermalise(g, a.therm)
+    # mixed form, timed
+    dist.barrier()
+    clocks = Clocks(dist.local)
+    acc, plaq, w, ms = time_cycles(g, eps, a.steps, a.warmup, clocks)
+    dist.barrier()
+    ms_max = dist.max(ms)
+    value = links_per_step * a.steps * dist.world / (ms_max * 1e-3)
+    # breakdown and roofline of the dominant kernel
+    ms_sweep, ms_meas = kernel_split(g, eps)
+    pk = measured_peaks()
+    hbm = pk.get("hbm_gbs")
+    fp32 = peak(1)
+    fp64 = peak(0)
+    bytes_link_mixed = 2 * 9 * 8  # read + write one FP32 SU(3) link
+    pass_ms = ms_sweep / 16.0
+    units_per_launch = V // 16 * 4
+    achieved = units_per_launch * bytes_link_mixed / (pass_ms * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "kernel": "metropolis_pass_kernel<3,4,float>", "achieved": achieved,
+                "peak": hbm, "unit": "GB/s", "frac": (achieved / hbm) if hbm else None,
+                "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if hbm else "fallback 6650",
+                "traffic": None, "algorithmic_bytes_per_launch": units_per_launch * bytes_link_mixed,
+                "avg_launch_ms": pass_ms,
+                "cuda_core_peak_tflops": {"fp32": fp32, "fp64": fp64}}
+    e2e_dt, h2d, d2h = e2e_public_api(g, eps, max(2, a.steps // 2))
+    e2e_steps = max(2, a.steps // 2)
+    e2e = {"value": links_per_step * e2e_steps / e2e_dt, "unit": "link updates/s", "h2d_bytes_per_step": h2d,
+           "d2h_bytes_per_step": d2h,
+           "path": "klft_metropolis_sweeps + klft_plaquette + klft_wilson_loop_temporal per step, host wall clock"}
+    hl_dt, hb, db = e2e_host_lattice(g, eps, 2)
+    e2e_host = {"value": links_per_step * 2 / hl_dt, "unit": "link updates/s", "h2d_bytes_per_step": hb,
+                "d2h_bytes_per_step": db, "path": "upload links + cycle + download links per step"}
+    # FP64 form from the same thermalised configuration
+    fp64_line = None
+    if not a.no_fp64:
+        U = g.download()
+        g64 = klft_b200.GaugeField(L, 3, "fp64", "cold", 0)
+        g64.upload(U)
+        g64.set_stream(1234, dist.rank)
+        _, plaq64, _, ms64 = time_cycles(g64, eps, a.steps, a.warmup)
+        ms64 = dist.max(ms64)
+        s64, m64 = kernel_split(g64, eps, 2)
+        fp64_line = {"value": links_per_step * a.steps * dist.world / (ms64 * 1e-3), "ms_per_step": ms64 / a.steps,
+                     "ms_sweep": s64, "ms_measure": m64, "mean_plaquette": float(np.mean(plaq64))}
+        g64.close()
+    launches_per_step = 16 + 1 + 2 + 3 * 2  # passes + counter advance + plaquette(2) + 3 x wilson(2)
+    line = {
+        "metric": METRIC, "value": value, "unit": "link updates/s", "n_gpus": dist.world, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 links / f64 reductions", "data": "synthetic (seeded cold start, "
+        f"{a.therm} thermalisation sweeps)",
+        "config": {"workload": f"SU(3) 4D {a.L}^4 Metropolis beta=6 nHits=10 exp(i eps H) proposals "
+                               f"(eps={eps:.4f}), per step 1 sweep + plaquette + W_temp(L,T in 1..8)",
+                   "parallelism": f"replicas x{dist.world}",
+                   "l2": f"inputs larger than L2 ({V * 4 * 9 * 8 / 1e6:.0f} MB of FP32 links)"},
+        "breakdown_ms": {"sweep": ms_sweep, "measure": ms_meas},
+        "acceptance": float(np.mean(acc)), "mean_plaquette": float(np.mean(plaq)),
+        "fp64": fp64_line,
+        "roofline": roofline, "e2e": e2e, "e2e_host_lattice": e2e_host,
+        "clocks": clocks.summary(), "gpu_launches": launches_per_step * a.steps,
+    }
+    if dist.rank == 0 and dist.world == 1 and not a.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = cpu_baseline_reference(a.L)
+        except Exception as ex:  # reported, not fatal
+            line["cpu_baseline"] = {"error": str(ex)}
+    g.close()
+    return line
+
+
+def run_reference(a, dist: Dist):
+    """klft's own code (headers compiled unchanged on the project's OpenMP shim) on the host cores."""
+    if dist.rank != 0:
+        return None
+    from oracle.oracle import REF_SO, Lat, RefShim
+    if not os.path.exists(REF_SO):
+        return {"impl": "reference", "unavailable": "oracle/_ref/libklft_ref.so not built (reference sources absent at "
+                                                    "build time)"}
+    r = RefShim()
+    cores = r.set_threads(os.cpu_count() or 1)
+    lat = Lat(3, [a.L] * 4)
+    U = lat.field()
+    for c in range(3):
+        U[:, :, c, c] = 1.0
+    for k in range(a.warmup):
+        r.cycles(lat, U, BETA, 0.1, NHITS, 1, 1234, PAIRS, sweep0=k)
+    t0 = time.perf_counter()
+    for k in range(a.steps):
+        r.cycles(lat, U, BETA, 0.1, NHITS, 1, 1234, PAIRS, sweep0=a.warmup + k)
+    dt = time.perf_counter() - t0
+    v = lat.V * 4 * a.steps / dt
+    return {"metric": METRIC, "value": v, "unit": "link updates/s", "n_gpus": dist.world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": dt * 1e3 / a.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (cold start)", "impl": "reference",
+            "config": {"workload": f"SU(3) 4D {a.L}^4 Metropolis beta=6 nHits=10 (reference SU(3) proposal), per "
+                                   f"step 1 sweep + plaquette + W_temp(L,T in 1..8)", "parallelism": "host OpenMP"},
+            "cpu_baseline": {"value": v, "unit": "link updates/s", "cores": cores, "kind": "reference",
+                             "sample": f"{a.steps} full cycles of SU(3) {a.L}^4 on {cores} host threads"},
+            "e2e": {"value": v, "unit": "link updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    a = parse()
+    dist = Dist() if a.impl == "ours" else None
+    if a.impl == "reference":
+        rank = int(os.environ.get("RANK", "0"))
+        if rank != 0:
+            return 0
+
+        class _D:
+            rank, world = 0, 1
+        line = run_reference(a, _D())
+    else:
+        line = run_ours(a, dist)
+    if line is not None and (dist is None or dist.rank == 0):
+        print(json.dumps(line))
+    if dist:
+        dist.close()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,106 @@
+/* klft_b200.h -- C ABI of libklft_b200.so, the B200 (sm_100a) implementation of
+ * klft's lattice-gauge update-and-measure path.
+ *
+ * Conventions
+ *  - Every entry point returns klft_status; on failure klft_last_error() gives a
+ *    thread-local message.  No exception crosses the ABI.
+ *  - Opaque handles own device memory and one CUDA stream each.  Calls on one
+ *    handle are serialised by the library; distinct handles may be used from
+ *    different threads.  Calls return after their device work has completed.
+ *  - Host link buffers use the interchange layout
+ *        U[(((site*Nd + mu)*Nc + i)*Nc + j)*2 + {0: re, 1: im}]   (double)
+ *    with site = x0 + L0*(x1 + L1*(x2 + L2*x3)).
+ *  - There is no CPU fallback: without a usable CUDA device every call that
+ *    needs one fails with KLFT_ECUDA.
+ *
+ * Each declaration names the reference (aniketsen/klft) interface it replaces.
+ */
+#ifndef KLFT_B200_H
+#define KLFT_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  KLFT_OK = 0,
+  KLFT_EINVAL = 1,   /* bad argument                        */
+  KLFT_ENOMEM = 2,   /* device or host allocation failed    */
+  KLFT_ECUDA = 3,    /* CUDA runtime error / no device      */
+  KLFT_ETIMEOUT = 4, /* a bounded device wait gave up       */
+  KLFT_ENOTSUP = 5   /* combination not supported           */
+} klft_status;
+
+typedef enum { KLFT_PRECISION_FP64 = 0, KLFT_PRECISION_MIXED = 1 } klft_precision;
+typedef enum { KLFT_START_COLD = 0, KLFT_START_HOT = 1 } klft_start;
+/* SU(3) proposal: the reference Gram-Schmidt generator (SUN.hpp:192-251) or
+ * X = exp(i eps H), H hermitian traceless Gaussian.  U(1)/SU(2) always use the
+ * reference generators (SUN.hpp:163-189). */
+typedef enum { KLFT_PROPOSAL_REFERENCE = 0, KLFT_PROPOSAL_EXP = 1 } klft_proposal;
+
+typedef struct klft_lattice klft_lattice;
+
+/* Thread-local description of the last failure on this thread. */
+const char *klft_last_error(void);
+/* Library version (major*10000 + minor*100 + patch). */
+int klft_version(void);
+/* Number of visible CUDA devices. */
+klft_status klft_device_count(int *n);
+
+/* Create a gauge field of SU(nc) (nc = 1: U(1)) links on an ndims-dimensional
+ * periodic lattice with even extents L[0..ndims-1] on the current device.
+ * Replaces deviceGaugeField{,3D,2D}<Nd,Nc> construction (GaugeField.hpp:30-141,
+ * 241-344, 437-540) and the cold start of lib/Metropolis.cpp:79-81.
+ * start = COLD: identity links; HOT: Haar-random links from seed. */
+klft_status klft_lattice_create(int nc, int ndims, const int *L, int precision, int start, uint64_t seed,
+                                klft_lattice **out);
+klft_status klft_lattice_destroy(klft_lattice *lat);
+klft_status klft_lattice_info(const klft_lattice *lat, int *nc, int *ndims, int *L, int *precision,
+                              long long *volume);
+/* Random stream identity: seed and chain key the Philox stream; the sweep and
+ * trajectory counters are its step words (checkpoint = links + these). */
+klft_status klft_lattice_set_stream(klft_lattice *lat, uint64_t seed, uint64_t chain);
+klft_status klft_lattice_get_counters(klft_lattice *lat, uint32_t *sweep, uint32_t *trajectory);
+klft_status klft_lattice_set_counters(klft_lattice *lat, uint32_t sweep, uint32_t trajectory);
+/* Copy links from / to a host buffer in the interchange layout. */
+klft_status klft_lattice_upload(klft_lattice *lat, const double *host);
+klft_status klft_lattice_download(klft_lattice *lat, double *host);
+
+/* nsweeps Metropolis sweeps; acc_out[k] = acceptance of sweep k normalised as
+ * sweep_Metropolis does (Metropolis.hpp:118-178).  Replaces sweep_Metropolis. */
+klft_status klft_metropolis_sweeps(klft_lattice *lat, double beta, double delta, int nhits, int proposal,
+                                   double eps, int nsweeps, double *acc_out);
+
+/* GaugePlaquette<rank,Nc>(g, normalize=true) (GaugePlaquette.hpp:89-135). */
+klft_status klft_plaquette(klft_lattice *lat, double *out);
+/* WilsonLoop_mu_nu (WilsonLoop.hpp:170-245): out[k] = W(mu, nu, pairs[2k], pairs[2k+1]). */
+klft_status klft_wilson_loop_mu_nu(klft_lattice *lat, int mu, int nu, const int *pairs, int npairs, double *out);
+/* WilsonLoop_temporal (WilsonLoop.hpp:250-304): out[k] = W_temp(L = pairs[2k], T = pairs[2k+1]). */
+klft_status klft_wilson_loop_temporal(klft_lattice *lat, const int *pairs, int npairs, double *out);
+/* stapleField (Gauge_Util.hpp:27-97), any ndims; out in the interchange layout. */
+klft_status klft_staple_field(klft_lattice *lat, double *out);
+/* max over links of ||U^dagger U - 1||_F. */
+klft_status klft_unitarity(klft_lattice *lat, double *out);
+/* restoreSUN on every link (SUN.hpp:256-340), in FP64 for both precisions. */
+klft_status klft_reunitarize(klft_lattice *lat);
+
+/* ncycles update-and-measure cycles enqueued back to back on the handle's stream,
+ * as run_metropolis does them (Metropolis.hpp:204-218): one sweep, then (when
+ * asked) GaugePlaquette and WilsonLoop_temporal over npairs (L, T) pairs.
+ * acc_out[c], plaq_out[c], w_out[c*npairs + k] receive the results (each may be
+ * NULL); device_ms the CUDA-event time of the whole sequence. */
+klft_status klft_run_cycles(klft_lattice *lat, double beta, double delta, int nhits, int proposal, double eps,
+                            int ncycles, int measure_plaquette, const int *temporal_pairs, int npairs,
+                            double *acc_out, double *plaq_out, double *w_out, double *device_ms);
+
+/* Diagnostic with no reference counterpart: measured CUDA-core FMA throughput
+ * (dtype 0: FP64, 1: FP32) of the current device in TFLOP/s, the roofline
+ * denominator of this library's SU(N) kernels. */
+klft_status klft_peak_flops(int dtype, double *tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* KLFT_B200_H */

@@ -1,0 +1,296 @@
+"""klft_b200 -- B200-native lattice-gauge update-and-measure (klft's API).
+
+Python mirror of the reference's operator interface, over the C ABI of
+libklft_b200.so (include/klft_b200.h).  Names follow klft:
+
+* ``GaugeField``            deviceGaugeField{,3D,2D}<Nd,Nc> (GaugeField.hpp)
+* ``MetropolisParams``      Metropolis_Params.hpp:28-99
+* ``GaugeObservableParams`` GaugeObservable.hpp:31-61
+* ``sweep_Metropolis``      Metropolis.hpp:118-178
+* ``run_metropolis``        Metropolis.hpp:180-223
+* ``GaugePlaquette``        GaugePlaquette.hpp:89-135
+* ``WilsonLoop_mu_nu``      WilsonLoop.hpp:170-245
+* ``WilsonLoop_temporal``   WilsonLoop.hpp:250-304
+* ``measureGaugeObservables`` / ``flushAllGaugeObservables``  GaugeObservable.hpp:64-230
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import List, Sequence, Tuple
+
+import numpy as np
+
+from ._lib import KlftError, check, lib
+
+PRECISION = {"fp64": 0, "mixed": 1}
+START = {"cold": 0, "hot": 1}
+PROPOSAL = {"reference": 0, "exp": 1}
+
+__all__ = [
+    "GaugeField", "MetropolisParams", "GaugeObservableParams", "KlftError", "sweep_Metropolis",
+    "run_metropolis", "GaugePlaquette", "WilsonLoop_mu_nu", "WilsonLoop_temporal",
+    "measureGaugeObservables", "flushAllGaugeObservables", "device_count",
+]
+
+
+def device_count() -> int:
+    n = C.c_int(0)
+    lib().klft_device_count(C.byref(n))
+    return n.value
+
+
+def _pairs(pairs) -> np.ndarray:
+    return np.ascontiguousarray(np.array(pairs, dtype=np.int32).reshape(-1, 2))
+
+
+class GaugeField:
+    """A device-resident SU(Nc) (Nc = 1: U(1)) gauge field on a periodic lattice."""
+
+    def __init__(self, L: Sequence[int], nc: int, precision: str = "fp64", start: str = "cold", seed: int = 0):
+        self.L = [int(x) for x in L]
+        self.nd = len(self.L)
+        self.nc = int(nc)
+        self.precision = precision
+        self.V = int(np.prod(self.L))
+        Lc = (C.c_int * 4)(*(self.L + [1] * (4 - self.nd)))
+        h = C.c_void_p()
+        check(lib().klft_lattice_create(self.nc, self.nd, Lc, PRECISION[precision], START[start], seed, C.byref(h)))
+        self._h = h
+
+    # -- lifetime
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib().klft_lattice_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    # -- state
+    def shape(self):
+        return (self.V, self.nd, self.nc, self.nc)
+
+    def upload(self, U: np.ndarray) -> None:
+        a = np.ascontiguousarray(U, dtype=np.complex128)
+        assert a.size == self.V * self.nd * self.nc * self.nc
+        check(lib().klft_lattice_upload(self._h, a.ctypes.data_as(C.POINTER(C.c_double))))
+
+    def download(self) -> np.ndarray:
+        a = np.zeros(self.shape(), dtype=np.complex128)
+        check(lib().klft_lattice_download(self._h, a.ctypes.data_as(C.POINTER(C.c_double))))
+        return a
+
+    def set_stream(self, seed: int, chain: int = 0) -> None:
+        check(lib().klft_lattice_set_stream(self._h, seed, chain))
+
+    def counters(self) -> Tuple[int, int]:
+        s, t = C.c_uint32(), C.c_uint32()
+        check(lib().klft_lattice_get_counters(self._h, C.byref(s), C.byref(t)))
+        return s.value, t.value
+
+    def set_counters(self, sweep: int, trajectory: int = 0) -> None:
+        check(lib().klft_lattice_set_counters(self._h, sweep, trajectory))
+
+    # -- update
+    def metropolis(self, beta: float, delta: float, nhits: int, nsweeps: int = 1, proposal: str = "reference",
+                   eps: float = 0.0) -> np.ndarray:
+        acc = np.zeros(max(nsweeps, 1))
+        check(lib().klft_metropolis_sweeps(self._h, beta, delta, nhits, PROPOSAL[proposal], eps, nsweeps,
+                                           acc.ctypes.data_as(C.POINTER(C.c_double))))
+        return acc[:nsweeps]
+
+    # -- measure
+    def plaquette(self) -> float:
+        o = C.c_double()
+        check(lib().klft_plaquette(self._h, C.byref(o)))
+        return o.value
+
+    def wilson_loop_mu_nu(self, mu: int, nu: int, pairs) -> np.ndarray:
+        p = _pairs(pairs)
+        o = np.zeros(len(p))
+        check(lib().klft_wilson_loop_mu_nu(self._h, mu, nu, p.ctypes.data_as(C.POINTER(C.c_int)), len(p),
+                                           o.ctypes.data_as(C.POINTER(C.c_double))))
+        return o
+
+    def wilson_loop_temporal(self, pairs) -> np.ndarray:
+        p = _pairs(pairs)
+        o = np.zeros(len(p))
+        check(lib().klft_wilson_loop_temporal(self._h, p.ctypes.data_as(C.POINTER(C.c_int)), len(p),
+                                              o.ctypes.data_as(C.POINTER(C.c_double))))
+        return o
+
+    def staple_field(self) -> np.ndarray:
+        a = np.zeros(self.shape(), dtype=np.complex128)
+        check(lib().klft_staple_field(self._h, a.ctypes.data_as(C.POINTER(C.c_double))))
+        return a
+
+    def run_cycles(self, beta: float, delta: float, nhits: int, ncycles: int, proposal: str = "reference",
+                   eps: float = 0.0, measure_plaquette: bool = True, temporal_pairs=()):
+        """ncycles sweep+measure cycles back to back; returns (acc, plaq, W, device_ms)."""
+        p = _pairs(temporal_pairs) if len(temporal_pairs) else np.zeros((0, 2), dtype=np.int32)
+        acc = np.zeros(max(ncycles, 1))
+        plaq = np.zeros(max(ncycles, 1))
+        w = np.zeros((max(ncycles, 1), max(len(p), 1)))
+        ms = C.c_double()
+        dp = C.POINTER(C.c_double)
+        check(lib().klft_run_cycles(self._h, beta, delta, nhits, PROPOSAL[proposal], eps, ncycles,
+                                    int(measure_plaquette), p.ctypes.data_as(C.POINTER(C.c_int)), len(p),
+                                    acc.ctypes.data_as(dp), plaq.ctypes.data_as(dp), w.ctypes.data_as(dp),
+                                    C.byref(ms)))
+        return acc[:ncycles], plaq[:ncycles], w[:ncycles, :len(p)], ms.value
+
+    def unitarity(self) -> float:
+        o = C.c_double()
+        check(lib().klft_unitarity(self._h, C.byref(o)))
+        return o.value
+
+    def reunitarize(self) -> None:
+        check(lib().klft_reunitarize(self._h))
+
+
+# ------------------------------------------------------------------ reference-style API
+@dataclass
+class MetropolisParams:
+    """Metropolis_Params.hpp:28-99 (struct defaults); YAML defaults differ (InputParser.hpp:41-54)."""
+    Ndims: int = 4
+    L0: int = 4
+    L1: int = 4
+    L2: int = 4
+    L3: int = 4
+    nHits: int = 10
+    nSweep: int = 1000
+    seed: int = 1234
+    Nd: int = 4
+    Nc: int = 2
+    beta: float = 1.0
+    delta: float = 0.1
+    # additions (ignored by the reference parser): SU(3) proposal and precision
+    proposal: str = "reference"
+    eps: float = 0.0
+    precision: str = "fp64"
+    start: str = "cold"
+
+    def dims(self) -> List[int]:
+        return [self.L0, self.L1, self.L2, self.L3][: self.Ndims]
+
+
+@dataclass
+class GaugeObservableParams:
+    """GaugeObservable.hpp:31-61."""
+    measurement_interval: int = 0
+    measure_plaquette: bool = False
+    measure_wilson_loop_temporal: bool = False
+    measure_wilson_loop_mu_nu: bool = False
+    W_temp_L_T_pairs: List[Tuple[int, int]] = field(default_factory=list)
+    W_mu_nu_pairs: List[Tuple[int, int]] = field(default_factory=list)
+    W_Lmu_Lnu_pairs: List[Tuple[int, int]] = field(default_factory=list)
+    measurement_steps: List[int] = field(default_factory=list)
+    plaquette_measurements: List[float] = field(default_factory=list)
+    W_temp_measurements: List[list] = field(default_factory=list)
+    W_mu_nu_measurements: List[list] = field(default_factory=list)
+    plaquette_filename: str = ""
+    W_temp_filename: str = ""
+    W_mu_nu_filename: str = ""
+    write_to_file: bool = False
+
+
+def sweep_Metropolis(g: GaugeField, params: MetropolisParams) -> float:
+    return float(g.metropolis(params.beta, params.delta, params.nHits, 1, params.proposal, params.eps)[0])
+
+
+def GaugePlaquette(g: GaugeField) -> float:
+    return g.plaquette()
+
+
+def WilsonLoop_mu_nu(g: GaugeField, mu: int, nu: int, pairs) -> List[Tuple[float, float, float, float, float]]:
+    w = g.wilson_loop_mu_nu(mu, nu, pairs)
+    return [(float(mu), float(nu), float(p[0]), float(p[1]), float(x)) for p, x in zip(_pairs(pairs), w)]
+
+
+def WilsonLoop_temporal(g: GaugeField, pairs) -> List[Tuple[float, float, float]]:
+    w = g.wilson_loop_temporal(pairs)
+    return [(float(p[0]), float(p[1]), float(x)) for p, x in zip(_pairs(pairs), w)]
+
+
+def measureGaugeObservables(g: GaugeField, params: GaugeObservableParams, step: int) -> None:
+    """GaugeObservable.hpp:64-127: measures at nonzero multiples of the interval."""
+    if params.measurement_interval == 0 or step % params.measurement_interval != 0 or step == 0:
+        return
+    if params.measure_plaquette:
+        params.plaquette_measurements.append(GaugePlaquette(g))
+    if params.measure_wilson_loop_temporal:
+        params.W_temp_measurements.append(WilsonLoop_temporal(g, params.W_temp_L_T_pairs))
+    if params.measure_wilson_loop_mu_nu:
+        rows = []
+        for mu, nu in params.W_mu_nu_pairs:
+            rows += WilsonLoop_mu_nu(g, mu, nu, params.W_Lmu_Lnu_pairs)
+        params.W_mu_nu_measurements.append(rows)
+    params.measurement_steps.append(step)
+
+
+def _fmt(x: float) -> str:
+    """Default std::ostream formatting of a double (6 significant digits, %g)."""
+    return "%g" % x
+
+
+def flushAllGaugeObservables(params: GaugeObservableParams, header: bool = True) -> None:
+    """GaugeObservable.hpp:130-230: append the measurements to their files."""
+    if not params.write_to_file:
+        print("write_to_file is not enabled")
+        return
+    if params.plaquette_filename:
+        with open(params.plaquette_filename, "a") as f:
+            if not params.measure_plaquette:
+                print("Error: no plaquette measurements available")
+            else:
+                if header:
+                    f.write("# step, plaquette\n")
+                for s, p in zip(params.measurement_steps, params.plaquette_measurements):
+                    f.write(f"{s}, {_fmt(p)}\n")
+    if params.W_temp_filename:
+        with open(params.W_temp_filename, "a") as f:
+            if not params.measure_wilson_loop_temporal:
+                print("Error: no temporal Wilson loop measurements available")
+            else:
+                if header:
+                    f.write("# step, L, T, W_temp\n")
+                for s, rows in zip(params.measurement_steps, params.W_temp_measurements):
+                    for r in rows:
+                        f.write(f"{s}, {_fmt(r[0])}, {_fmt(r[1])}, {_fmt(r[2])}\n")
+    if params.W_mu_nu_filename:
+        with open(params.W_mu_nu_filename, "a") as f:
+            if not params.measure_wilson_loop_mu_nu:
+                print("Error: no mu-nu Wilson loop measurements available")
+            else:
+                if header:
+                    f.write("# step, mu, nu, Lmu, Lnu, W_mu_nu\n")
+                for s, rows in zip(params.measurement_steps, params.W_mu_nu_measurements):
+                    for r in rows:
+                        f.write(f"{s}, " + ", ".join(_fmt(v) for v in r) + "\n")
+
+
+def run_metropolis(g: GaugeField, mp: MetropolisParams, op: GaugeObservableParams, verbosity: int = 0) -> int:
+    """Metropolis.hpp:180-223."""
+    import time
+    for step in range(mp.nSweep):
+        t0 = time.perf_counter()
+        acc = sweep_Metropolis(g, mp)
+        if verbosity > 0:
+            print("Step: %d, Acceptance rate: %f, Time: %f" % (step, acc, time.perf_counter() - t0))
+        measureGaugeObservables(g, op, step)
+    flushAllGaugeObservables(op)
+    return 0

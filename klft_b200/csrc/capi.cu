@@ -1,0 +1,494 @@
+// capi.cu -- the extern "C" boundary of libklft_b200.so (declared in
+// include/klft_b200.h): lattice handles, their streams and scratch, and the
+// host-side sequencing of the kernels (sweep = 2^Nd parity-class passes).
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/klft_b200.h"
+#include "capi_internal.h"
+#include "kernels.cuh"
+
+using namespace klft;
+
+namespace klft {
+
+static thread_local std::string g_last_error;
+
+klft_status fail(klft_status code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+klft_status cuda_fail(cudaError_t e, const char *what) {
+  return fail(e == cudaErrorMemoryAllocation ? KLFT_ENOMEM : KLFT_ECUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+cudaError_t Scratch::ensure(size_t bytes) {
+  if (bytes <= cap) return cudaSuccess;
+  if (ptr) cudaFree(ptr);
+  ptr = nullptr;
+  cap = 0;
+  cudaError_t e = cudaMalloc(&ptr, bytes);
+  if (e == cudaSuccess) cap = bytes;
+  return e;
+}
+void Scratch::release() {
+  if (ptr) cudaFree(ptr);
+  ptr = nullptr;
+  cap = 0;
+}
+
+}  // namespace klft
+
+#define CK(call)                                           \
+  do {                                                     \
+    cudaError_t e_ = (call);                               \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call);    \
+  } while (0)
+
+#define LOCK(lat) std::lock_guard<std::mutex> guard_((lat)->mtx)
+
+static size_t elem_bytes(int precision) { return precision == KLFT_PRECISION_FP64 ? 16 : 8; }
+
+klft_status klft::lattice_sync(klft_lattice *lat) {
+  CK(cudaStreamSynchronize(lat->stream));
+  return KLFT_OK;
+}
+
+// Proposal arguments: the reference SU(3) generator needs delta > 0 (its
+// rejection loops draw from [0, delta) until the norm is nonzero).
+static klft_status check_proposal(const klft_lattice *lat, double delta, int proposal, double eps, const char *who) {
+  if (proposal != KLFT_PROPOSAL_REFERENCE && proposal != KLFT_PROPOSAL_EXP)
+    return fail(KLFT_EINVAL, "%s: unknown proposal %d", who, proposal);
+  if (!(delta == delta) || !(eps == eps)) return fail(KLFT_EINVAL, "%s: NaN step size", who);
+  if (lat->nc == 3 && proposal == KLFT_PROPOSAL_REFERENCE && !(delta > 0.0))
+    return fail(KLFT_EINVAL, "%s: the reference SU(3) proposal needs delta > 0 (got %g)", who, delta);
+  return KLFT_OK;
+}
+
+extern "C" {
+
+const char *klft_last_error(void) { return g_last_error.c_str(); }
+
+int klft_version(void) { return 100; }
+
+klft_status klft_device_count(int *n) {
+  if (!n) return fail(KLFT_EINVAL, "klft_device_count: null pointer");
+  cudaError_t e = cudaGetDeviceCount(n);
+  if (e != cudaSuccess) {
+    *n = 0;
+    return cuda_fail(e, "cudaGetDeviceCount");
+  }
+  return KLFT_OK;
+}
+
+klft_status klft_lattice_create(int nc, int ndims, const int *L, int precision, int start, uint64_t seed,
+                                klft_lattice **out) {
+  if (!out || !L) return fail(KLFT_EINVAL, "klft_lattice_create: null pointer");
+  *out = nullptr;
+  if (nc < 1 || nc > 3) return fail(KLFT_EINVAL, "klft_lattice_create: Nc must be 1, 2 or 3 (got %d)", nc);
+  if (ndims < 2 || ndims > 4) return fail(KLFT_EINVAL, "klft_lattice_create: ndims must be 2, 3 or 4 (got %d)", ndims);
+  if (precision != KLFT_PRECISION_FP64 && precision != KLFT_PRECISION_MIXED)
+    return fail(KLFT_EINVAL, "klft_lattice_create: unknown precision %d", precision);
+  if (start != KLFT_START_COLD && start != KLFT_START_HOT)
+    return fail(KLFT_EINVAL, "klft_lattice_create: unknown start %d", start);
+  long long V = 1;
+  for (int d = 0; d < ndims; ++d) {
+    if (L[d] < 2 || (L[d] & 1))
+      return fail(KLFT_EINVAL, "klft_lattice_create: extent L%d = %d must be even and >= 2", d, L[d]);
+    V *= L[d];
+  }
+  if (V > 0x7fffffffLL) return fail(KLFT_EINVAL, "klft_lattice_create: volume %lld exceeds 2^31-1", V);
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0) return fail(KLFT_ECUDA, "klft_lattice_create: no CUDA device available");
+
+  klft_lattice *lat = new klft_lattice();
+  lat->nc = nc;
+  lat->precision = precision;
+  lat->seed = seed;
+  lat->chain = 0;
+  Geom &g = lat->g;
+  g.nd = ndims;
+  long long Vh = 1;
+  int stride = 1;
+  for (int d = 0; d < 4; ++d) {
+    g.L[d] = d < ndims ? L[d] : 1;
+    g.H[d] = d < ndims ? L[d] / 2 : 1;
+    g.hs[d] = stride;
+    stride *= g.H[d];
+    Vh *= g.H[d];
+  }
+  g.V = V;
+  g.Vh = Vh;
+  // lattices with a singleton parity dimension keep the 2-class structure per dim
+  cudaGetDevice(&lat->device);
+  lat->link_bytes = (size_t)V * ndims * nc * nc * elem_bytes(precision);
+  e = cudaStreamCreateWithFlags(&lat->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) { delete lat; return cuda_fail(e, "cudaStreamCreate"); }
+  e = cudaMalloc(&lat->links, lat->link_bytes);
+  if (e != cudaSuccess) {
+    cudaStreamDestroy(lat->stream);
+    delete lat;
+    return cuda_fail(e, "cudaMalloc(links)");
+  }
+  e = cudaMalloc(&lat->d_counters, 4 * sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaMemsetAsync(lat->d_counters, 0, 4 * sizeof(uint32_t), lat->stream);
+  if (e == cudaSuccess) e = cudaMallocHost(&lat->h_results, KLFT_RESULT_SLOTS * sizeof(double));
+  if (e == cudaSuccess)
+    e = launch_init(nc, precision == KLFT_PRECISION_FP64 ? 0 : 1, lat->links, g, start == KLFT_START_HOT, seed, 0,
+                    lat->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(lat->stream);
+  if (e != cudaSuccess) {
+    klft_status s = cuda_fail(e, "klft_lattice_create");
+    klft_lattice_destroy(lat);
+    return s;
+  }
+  *out = lat;
+  return KLFT_OK;
+}
+
+klft_status klft_lattice_destroy(klft_lattice *lat) {
+  if (!lat) return KLFT_OK;
+  {
+    LOCK(lat);
+    if (lat->stream) cudaStreamSynchronize(lat->stream);
+    for (Scratch *s : {&lat->s_part, &lat->s_out, &lat->s_aux, &lat->s_stage, &lat->s_wl, &lat->s_hmc})
+      s->release();
+    if (lat->links) cudaFree(lat->links);
+    if (lat->d_counters) cudaFree(lat->d_counters);
+    if (lat->h_results) cudaFreeHost(lat->h_results);
+    if (lat->stream) cudaStreamDestroy(lat->stream);
+  }
+  delete lat;
+  return KLFT_OK;
+}
+
+klft_status klft_lattice_info(const klft_lattice *lat, int *nc, int *ndims, int *L, int *precision,
+                              long long *volume) {
+  if (!lat) return fail(KLFT_EINVAL, "klft_lattice_info: null handle");
+  if (nc) *nc = lat->nc;
+  if (ndims) *ndims = lat->g.nd;
+  if (L)
+    for (int d = 0; d < lat->g.nd; ++d) L[d] = lat->g.L[d];
+  if (precision) *precision = lat->precision;
+  if (volume) *volume = lat->g.V;
+  return KLFT_OK;
+}
+
+klft_status klft_lattice_set_stream(klft_lattice *lat, uint64_t seed, uint64_t chain) {
+  if (!lat) return fail(KLFT_EINVAL, "klft_lattice_set_stream: null handle");
+  LOCK(lat);
+  lat->seed = seed;
+  lat->chain = chain;
+  return KLFT_OK;
+}
+
+klft_status klft_lattice_get_counters(klft_lattice *lat, uint32_t *sweep, uint32_t *trajectory) {
+  if (!lat) return fail(KLFT_EINVAL, "klft_lattice_get_counters: null handle");
+  LOCK(lat);
+  uint32_t c[4];
+  CK(cudaMemcpyAsync(c, lat->d_counters, sizeof c, cudaMemcpyDeviceToHost, lat->stream));
+  CK(cudaStreamSynchronize(lat->stream));
+  if (sweep) *sweep = c[0];
+  if (trajectory) *trajectory = c[1];
+  return KLFT_OK;
+}
+
+klft_status klft_lattice_set_counters(klft_lattice *lat, uint32_t sweep, uint32_t trajectory) {
+  if (!lat) return fail(KLFT_EINVAL, "klft_lattice_set_counters: null handle");
+  LOCK(lat);
+  uint32_t c[4] = {sweep, trajectory, 0, 0};
+  CK(cudaMemcpyAsync(lat->d_counters, c, sizeof c, cudaMemcpyHostToDevice, lat->stream));
+  CK(cudaStreamSynchronize(lat->stream));
+  return KLFT_OK;
+}
+
+klft_status klft_lattice_upload(klft_lattice *lat, const double *host) {
+  if (!lat || !host) return fail(KLFT_EINVAL, "klft_lattice_upload: null pointer");
+  LOCK(lat);
+  const size_t bytes = (size_t)lat->g.V * lat->g.nd * lat->nc * lat->nc * 16;
+  CK(lat->s_stage.ensure(bytes));
+  CK(cudaMemcpyAsync(lat->s_stage.ptr, host, bytes, cudaMemcpyHostToDevice, lat->stream));
+  CK(launch_import(lat->nc, lat->dtype(), lat->links, lat->g, (const double *)lat->s_stage.ptr, lat->stream));
+  CK(cudaStreamSynchronize(lat->stream));
+  return KLFT_OK;
+}
+
+klft_status klft_lattice_download(klft_lattice *lat, double *host) {
+  if (!lat || !host) return fail(KLFT_EINVAL, "klft_lattice_download: null pointer");
+  LOCK(lat);
+  const size_t bytes = (size_t)lat->g.V * lat->g.nd * lat->nc * lat->nc * 16;
+  CK(lat->s_stage.ensure(bytes));
+  CK(launch_export(lat->nc, lat->dtype(), lat->links, lat->g, (double *)lat->s_stage.ptr, lat->stream));
+  CK(cudaMemcpyAsync(host, lat->s_stage.ptr, bytes, cudaMemcpyDeviceToHost, lat->stream));
+  CK(cudaStreamSynchronize(lat->stream));
+  return KLFT_OK;
+}
+
+klft_status klft_metropolis_sweeps(klft_lattice *lat, double beta, double delta, int nhits, int proposal, double eps,
+                                   int nsweeps, double *acc_out) {
+  if (!lat) return fail(KLFT_EINVAL, "klft_metropolis_sweeps: null handle");
+  if (nhits < 0 || nsweeps < 0) return fail(KLFT_EINVAL, "klft_metropolis_sweeps: negative count");
+  klft_status v = check_proposal(lat, delta, proposal, eps, "klft_metropolis_sweeps");
+  if (v != KLFT_OK) return v;
+  if (nsweeps == 0) return KLFT_OK;
+  LOCK(lat);
+  CK(lat->s_aux.ensure((size_t)nsweeps * sizeof(unsigned long long)));
+  unsigned long long *d_nacc = (unsigned long long *)lat->s_aux.ptr;
+  CK(cudaMemsetAsync(d_nacc, 0, (size_t)nsweeps * sizeof(unsigned long long), lat->stream));
+  klft_status s = enqueue_sweeps(lat, beta, delta, nhits, proposal, eps, nsweeps, d_nacc, lat->defect);
+  if (s != KLFT_OK) return s;
+  if (acc_out) {
+    std::vector<unsigned long long> h(nsweeps);
+    CK(cudaMemcpyAsync(h.data(), d_nacc, (size_t)nsweeps * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                       lat->stream));
+    CK(cudaStreamSynchronize(lat->stream));
+    double norm = 1.0;
+    for (int d = 0; d < lat->g.nd; ++d) norm *= (double)lat->g.L[d];
+    norm *= (double)lat->g.nd;
+    norm *= (double)nhits;
+    for (int k = 0; k < nsweeps; ++k) acc_out[k] = nhits > 0 ? (double)h[k] / norm : 0.0;
+  } else {
+    CK(cudaStreamSynchronize(lat->stream));
+  }
+  return KLFT_OK;
+}
+
+klft_status klft_plaquette(klft_lattice *lat, double *out) {
+  if (!lat || !out) return fail(KLFT_EINVAL, "klft_plaquette: null pointer");
+  LOCK(lat);
+  klft_status s = enqueue_plaquette(lat, 0);
+  if (s != KLFT_OK) return s;
+  CK(cudaMemcpyAsync(lat->h_results, lat->s_out.ptr, sizeof(double), cudaMemcpyDeviceToHost, lat->stream));
+  CK(cudaStreamSynchronize(lat->stream));
+  *out = normalize_plaquette(lat, lat->h_results[0]);
+  return KLFT_OK;
+}
+
+klft_status klft_wilson_loop_mu_nu(klft_lattice *lat, int mu, int nu, const int *pairs, int npairs, double *out) {
+  if (!lat || (npairs > 0 && (!pairs || !out))) return fail(KLFT_EINVAL, "klft_wilson_loop_mu_nu: null pointer");
+  if (mu < 0 || nu < 0 || mu >= lat->g.nd || nu >= lat->g.nd || mu == nu)
+    return fail(KLFT_EINVAL, "klft_wilson_loop_mu_nu: bad plane (%d, %d)", mu, nu);
+  for (int k = 0; k < npairs; ++k)
+    if (pairs[2 * k] < 0 || pairs[2 * k + 1] < 0)
+      return fail(KLFT_EINVAL, "klft_wilson_loop_mu_nu: negative loop extent");
+  if (npairs == 0) return KLFT_OK;
+  LOCK(lat);
+  std::vector<double> sums(npairs);
+  klft_status s = wilson_sums(lat, mu, nu, pairs, npairs, sums.data());
+  if (s != KLFT_OK) return s;
+  for (int k = 0; k < npairs; ++k) out[k] = normalize_wilson(lat, sums[k]);
+  return KLFT_OK;
+}
+
+klft_status klft_wilson_loop_temporal(klft_lattice *lat, const int *pairs, int npairs, double *out) {
+  if (!lat || (npairs > 0 && (!pairs || !out))) return fail(KLFT_EINVAL, "klft_wilson_loop_temporal: null pointer");
+  for (int k = 0; k < npairs; ++k)
+    if (pairs[2 * k] < 0 || pairs[2 * k + 1] < 0)
+      return fail(KLFT_EINVAL, "klft_wilson_loop_temporal: negative loop extent");
+  if (npairs == 0) return KLFT_OK;
+  LOCK(lat);
+  const int nd = lat->g.nd;
+  std::vector<double> acc(npairs, 0.0), sums(npairs);
+  for (int mu = 0; mu < nd - 1; ++mu) {
+    klft_status s = wilson_sums(lat, mu, nd - 1, pairs, npairs, sums.data());
+    if (s != KLFT_OK) return s;
+    for (int k = 0; k < npairs; ++k) {
+      const double w = normalize_wilson(lat, sums[k]);
+      acc[k] = mu == 0 ? w : acc[k] + w;
+    }
+  }
+  for (int k = 0; k < npairs; ++k) out[k] = acc[k] / (double)(nd - 1);
+  return KLFT_OK;
+}
+
+klft_status klft_staple_field(klft_lattice *lat, double *out) {
+  if (!lat || !out) return fail(KLFT_EINVAL, "klft_staple_field: null pointer");
+  LOCK(lat);
+  const size_t bytes = (size_t)lat->g.V * lat->g.nd * lat->nc * lat->nc * 16;
+  CK(lat->s_stage.ensure(bytes));
+  CK(launch_staple_field(lat->nc, lat->dtype(), lat->links, lat->g, (double *)lat->s_stage.ptr, lat->stream));
+  CK(cudaMemcpyAsync(out, lat->s_stage.ptr, bytes, cudaMemcpyDeviceToHost, lat->stream));
+  CK(cudaStreamSynchronize(lat->stream));
+  return KLFT_OK;
+}
+
+klft_status klft_unitarity(klft_lattice *lat, double *out) {
+  if (!lat || !out) return fail(KLFT_EINVAL, "klft_unitarity: null pointer");
+  LOCK(lat);
+  CK(lat->s_part.ensure(4096 * sizeof(double)));
+  CK(lat->s_out.ensure(KLFT_RESULT_SLOTS * sizeof(double)));
+  CK(launch_unitarity(lat->nc, lat->dtype(), lat->links, lat->g, (double *)lat->s_part.ptr, (double *)lat->s_out.ptr,
+                      lat->stream));
+  CK(cudaMemcpyAsync(lat->h_results, lat->s_out.ptr, sizeof(double), cudaMemcpyDeviceToHost, lat->stream));
+  CK(cudaStreamSynchronize(lat->stream));
+  *out = lat->h_results[0];
+  return KLFT_OK;
+}
+
+klft_status klft_reunitarize(klft_lattice *lat) {
+  if (!lat) return fail(KLFT_EINVAL, "klft_reunitarize: null handle");
+  LOCK(lat);
+  CK(launch_reunitarize(lat->nc, lat->dtype(), lat->links, lat->g, lat->stream));
+  CK(cudaStreamSynchronize(lat->stream));
+  return KLFT_OK;
+}
+
+klft_status klft_run_cycles(klft_lattice *lat, double beta, double delta, int nhits, int proposal, double eps,
+                            int ncycles, int measure_plaquette, const int *temporal_pairs, int npairs,
+                            double *acc_out, double *plaq_out, double *w_out, double *device_ms) {
+  if (!lat) return fail(KLFT_EINVAL, "klft_run_cycles: null handle");
+  if (ncycles < 0 || nhits < 0 || npairs < 0) return fail(KLFT_EINVAL, "klft_run_cycles: negative count");
+  if (npairs > 0 && !temporal_pairs) return fail(KLFT_EINVAL, "klft_run_cycles: null pairs");
+  klft_status v = check_proposal(lat, delta, proposal, eps, "klft_run_cycles");
+  if (v != KLFT_OK) return v;
+  for (int k = 0; k < npairs; ++k)
+    if (temporal_pairs[2 * k] < 0 || temporal_pairs[2 * k + 1] < 0)
+      return fail(KLFT_EINVAL, "klft_run_cycles: negative loop extent");
+  if (ncycles == 0) return KLFT_OK;
+  LOCK(lat);
+  const int nd = lat->g.nd;
+  const int nw = (nd - 1) * npairs;  // per cycle: one sum per (spatial mu, pair)
+  // aux layout: [pairs (2*npairs int, padded)] [nacc (ncycles u64)] ; out layout: [plaq ncycles][w ncycles*nw]
+  const size_t pair_bytes = ((size_t)npairs * 2 * sizeof(int) + 15) & ~(size_t)15;
+  CK(lat->s_aux.ensure(pair_bytes + (size_t)ncycles * sizeof(unsigned long long)));
+  CK(lat->s_wl.ensure((size_t)ncycles * (1 + nw) * sizeof(double)));
+  int *d_pairs = (int *)lat->s_aux.ptr;
+  unsigned long long *d_nacc = (unsigned long long *)((char *)lat->s_aux.ptr + pair_bytes);
+  double *d_plaq = (double *)lat->s_wl.ptr;
+  double *d_w = d_plaq + ncycles;
+  if (npairs > 0)
+    CK(cudaMemcpyAsync(d_pairs, temporal_pairs, (size_t)npairs * 2 * sizeof(int), cudaMemcpyHostToDevice,
+                       lat->stream));
+  CK(cudaMemsetAsync(d_nacc, 0, (size_t)ncycles * sizeof(unsigned long long), lat->stream));
+  {
+    const int nblk = plaquette_blocks(lat->g);
+    CK(lat->s_part.ensure((size_t)nblk * (npairs > 1 ? npairs : 1) * sizeof(double)));
+  }
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  CK(cudaEventRecord(e0, lat->stream));
+  for (int c = 0; c < ncycles; ++c) {
+    klft_status s = enqueue_sweeps(lat, beta, delta, nhits, proposal, eps, 1, d_nacc + c, lat->defect);
+    if (s != KLFT_OK) return s;
+    if (measure_plaquette) {
+      const int nblk = plaquette_blocks(lat->g);
+      CK(lat->s_part.ensure((size_t)nblk * sizeof(double)));
+      CK(launch_plaquette(lat->nc, lat->dtype(), lat->links, lat->g, (double *)lat->s_part.ptr, nblk, d_plaq + c,
+                          lat->stream));
+    }
+    for (int mu = 0; mu < nd - 1 && npairs > 0; ++mu) {
+      s = enqueue_wilson(lat, mu, nd - 1, d_pairs, npairs, d_w + (size_t)c * nw + (size_t)mu * npairs);
+      if (s != KLFT_OK) return s;
+    }
+  }
+  CK(cudaEventRecord(e1, lat->stream));
+  std::vector<unsigned long long> h_nacc(ncycles);
+  std::vector<double> h_out((size_t)ncycles * (1 + nw));
+  CK(cudaMemcpyAsync(h_nacc.data(), d_nacc, (size_t)ncycles * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                     lat->stream));
+  CK(cudaMemcpyAsync(h_out.data(), d_plaq, h_out.size() * sizeof(double), cudaMemcpyDeviceToHost, lat->stream));
+  CK(cudaStreamSynchronize(lat->stream));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (device_ms) *device_ms = ms;
+  double norm = 1.0;
+  for (int d = 0; d < nd; ++d) norm *= (double)lat->g.L[d];
+  norm *= (double)nd;
+  norm *= (double)nhits;
+  for (int c = 0; c < ncycles; ++c) {
+    if (acc_out) acc_out[c] = nhits > 0 ? (double)h_nacc[c] / norm : 0.0;
+    if (plaq_out && measure_plaquette) plaq_out[c] = normalize_plaquette(lat, h_out[c]);
+    if (w_out)
+      for (int k = 0; k < npairs; ++k) {
+        double acc = 0.0;
+        for (int mu = 0; mu < nd - 1; ++mu) {
+          const double w = normalize_wilson(lat, h_out[ncycles + (size_t)c * nw + (size_t)mu * npairs + k]);
+          acc = mu == 0 ? w : acc + w;
+        }
+        w_out[(size_t)c * npairs + k] = acc / (double)(nd - 1);
+      }
+  }
+  return KLFT_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ enqueue helpers
+namespace klft {
+
+klft_status enqueue_sweeps(klft_lattice *lat, double beta, double delta, int nhits, int proposal, double eps,
+                           int nsweeps, unsigned long long *d_nacc, const Defect &df) {
+  MetroArgs a{beta, delta, eps, nhits, proposal, lat->seed, lat->chain};
+  const int nclass = 1 << lat->g.nd;
+  for (int k = 0; k < nsweeps; ++k) {
+    for (int val = 0; val < nclass; ++val)
+      CK(launch_metropolis_pass(lat->nc, lat->dtype(), lat->links, lat->g, val, a, lat->d_counters, d_nacc + k, df, 0,
+                                lat->stream));
+    CK(launch_advance(lat->d_counters, lat->stream));
+  }
+  return KLFT_OK;
+}
+
+klft_status enqueue_plaquette(klft_lattice *lat, int slot) {
+  const int nblk = plaquette_blocks(lat->g);
+  CK(lat->s_part.ensure((size_t)nblk * sizeof(double)));
+  CK(lat->s_out.ensure(KLFT_RESULT_SLOTS * sizeof(double)));
+  CK(launch_plaquette(lat->nc, lat->dtype(), lat->links, lat->g, (double *)lat->s_part.ptr, nblk,
+                      (double *)lat->s_out.ptr + slot, lat->stream));
+  return KLFT_OK;
+}
+
+double normalize_plaquette(const klft_lattice *lat, double sum) {
+  // GaugePlaquette.hpp:125-132
+  double norm = 1.0;
+  for (int d = 0; d < lat->g.nd; ++d) norm *= (double)lat->g.L[d];
+  norm *= (double)((lat->g.nd * (lat->g.nd - 1) / 2) * lat->nc);
+  return sum / norm;
+}
+
+double normalize_wilson(const klft_lattice *lat, double sum) {
+  // WilsonLoop.hpp:233-240
+  double w = sum;
+  for (int d = 0; d < lat->g.nd; ++d) w /= (double)lat->g.L[d];
+  w /= (double)lat->nc;
+  return w;
+}
+
+// enqueue: d_out[k] = unnormalised sum over sites of Re Tr W for pair k (device pairs)
+klft_status enqueue_wilson(klft_lattice *lat, int mu, int nu, const int *d_pairs, int npairs, double *d_out) {
+  const int nblk = plaquette_blocks(lat->g);
+  CK(lat->s_part.ensure((size_t)nblk * npairs * sizeof(double)));
+  CK(launch_wilson_direct(lat->nc, lat->dtype(), lat->links, lat->g, mu, nu, d_pairs, npairs,
+                          (double *)lat->s_part.ptr, nblk, d_out, lat->stream));
+  return KLFT_OK;
+}
+
+// unnormalised sums over sites for a list of (Lmu, Lnu) pairs in the (mu, nu) plane
+klft_status wilson_sums(klft_lattice *lat, int mu, int nu, const int *pairs, int npairs, double *sums) {
+  CK(lat->s_out.ensure((size_t)(npairs > KLFT_RESULT_SLOTS ? npairs : KLFT_RESULT_SLOTS) * sizeof(double)));
+  CK(lat->s_aux.ensure((size_t)npairs * 2 * sizeof(int)));
+  CK(cudaMemcpyAsync(lat->s_aux.ptr, pairs, (size_t)npairs * 2 * sizeof(int), cudaMemcpyHostToDevice, lat->stream));
+  klft_status s = enqueue_wilson(lat, mu, nu, (const int *)lat->s_aux.ptr, npairs, (double *)lat->s_out.ptr);
+  if (s != KLFT_OK) return s;
+  CK(cudaMemcpyAsync(sums, lat->s_out.ptr, (size_t)npairs * sizeof(double), cudaMemcpyDeviceToHost, lat->stream));
+  CK(cudaStreamSynchronize(lat->stream));
+  return KLFT_OK;
+}
+
+}  // namespace klft

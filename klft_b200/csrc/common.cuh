@@ -1,0 +1,386 @@
+// common.cuh -- device building blocks shared by all kernels of libklft_b200:
+// the counter-based random stream, complex and SU(N) matrix algebra templated on
+// the storage/arithmetic type T (double: plain FP64 form, float: mixed form),
+// and the site geometry of the sublattice-blocked link layout.
+//
+// Link layout in HBM (structure of arrays, sublattice blocked):
+//   element (site x, direction mu, colour entry c = i*Nc + j) lives at
+//     links[(mu*Nc*Nc + c) * V + lin(x)]        as a complex of T
+//   lin(x) = sub(x) * Vh + hidx(x)
+//   sub(x) = sum_d (x_d & 1) << d                (2^Nd parity classes)
+//   hidx(x) = h0 + H0*(h1 + H1*(h2 + H2*h3)),  h_d = x_d >> 1,  H_d = L_d / 2
+// A parity class is contiguous, so a sublattice pass (the unit of the
+// reference's sweep, Metropolis.hpp:139-164) reads its own links and those of
+// its neighbours with unit-stride, fully coalesced accesses.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace klft {
+
+#define KLFT_HD __host__ __device__ __forceinline__
+#define KLFT_D __device__ __forceinline__
+
+// ------------------------------------------------------------------ random
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11).
+KLFT_HD void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+#ifdef __CUDA_ARCH__
+    const uint32_t hi0 = __umulhi(0xD2511F53u, c[0]), lo0 = 0xD2511F53u * c[0];
+    const uint32_t hi1 = __umulhi(0xCD9E8D57u, c[2]), lo1 = 0xCD9E8D57u * c[2];
+#else
+    const uint64_t p0 = (uint64_t)0xD2511F53u * c[0], p1 = (uint64_t)0xCD9E8D57u * c[2];
+    const uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0, hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+#endif
+    const uint32_t n0 = hi1 ^ c[1] ^ k0, n2 = hi0 ^ c[3] ^ k1;
+    c[0] = n0; c[1] = lo1; c[2] = n2; c[3] = lo0;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+}
+
+enum StreamKind : uint32_t {
+  KIND_METROPOLIS = 1u,  // per (sweep, site): Nd links x nHits hits, in order
+  KIND_INIT = 2u,        // per (site, mu): hot-start link
+  KIND_MOMENTUM = 3u,    // per (trajectory, site, mu): HMC momenta
+  KIND_HMC_ACCEPT = 4u,  // per trajectory: accept/reject uniform
+  KIND_SWAP = 5u,        // per (cycle, pair): replica swap uniform
+};
+
+// Sequential stream of 53-bit uniforms in [0,1).  key = (lo32(seed),
+// hi32(seed) ^ lo32(chain)), counter = (block, site, step, kind<<24 | sub).
+// Each Philox block gives two doubles, (w0:w1) then (w2:w3).
+struct Stream {
+  uint32_t k0, k1, site, step, tag, block;
+  uint32_t w[4];
+  int avail;
+  KLFT_HD Stream(uint64_t seed, uint64_t chain, uint32_t site_, uint32_t step_, uint32_t kind, uint32_t sub)
+      : k0((uint32_t)seed), k1((uint32_t)(seed >> 32) ^ (uint32_t)chain), site(site_), step(step_),
+        tag((kind << 24) | (sub & 0xFFFFFFu)), block(0), avail(0) {}
+  KLFT_HD double next() {
+    if (avail == 0) {
+      w[0] = block; w[1] = site; w[2] = step; w[3] = tag;
+      philox4x32_10(w, k0, k1);
+      ++block;
+      avail = 2;
+    }
+    const uint32_t hi = avail == 2 ? w[0] : w[2];
+    const uint32_t lo = avail == 2 ? w[1] : w[3];
+    --avail;
+    return (double)((((uint64_t)hi << 32) | lo) >> 11) * 0x1.0p-53;
+  }
+  // Kokkos drand(start, end) = start + (end - start) * u
+  KLFT_HD double drand(double a, double b) { return a + (b - a) * next(); }
+  // Box-Muller pair
+  KLFT_D void gauss2(double &g0, double &g1) {
+    const double u0 = next(), u1 = next();
+    const double r = sqrt(-2.0 * log(1.0 - u0));
+    double s, c;
+    sincos(6.283185307179586 * u1, &s, &c);
+    g0 = r * c;
+    g1 = r * s;
+  }
+};
+
+// ------------------------------------------------------------------ complex
+template <typename T> struct cx { T re, im; };
+
+template <typename T> KLFT_HD cx<T> mk(T r, T i) { return cx<T>{r, i}; }
+template <typename T> KLFT_HD cx<T> operator+(cx<T> a, cx<T> b) { return {a.re + b.re, a.im + b.im}; }
+template <typename T> KLFT_HD cx<T> operator-(cx<T> a, cx<T> b) { return {a.re - b.re, a.im - b.im}; }
+template <typename T> KLFT_HD cx<T> operator*(cx<T> a, cx<T> b) {
+  return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+}
+template <typename T> KLFT_HD cx<T> operator*(cx<T> a, T s) { return {a.re * s, a.im * s}; }
+template <typename T> KLFT_HD cx<T> operator*(T s, cx<T> a) { return {s * a.re, s * a.im}; }
+template <typename T> KLFT_HD cx<T> conj(cx<T> a) { return {a.re, -a.im}; }
+template <typename T> KLFT_HD void operator+=(cx<T> &a, cx<T> b) { a.re += b.re; a.im += b.im; }
+template <typename T> KLFT_HD void operator-=(cx<T> &a, cx<T> b) { a.re -= b.re; a.im -= b.im; }
+// complex / real, as std::complex does it
+template <typename T> KLFT_HD cx<T> cdiv(cx<T> a, T s) { return {a.re / s, a.im / s}; }
+
+// ------------------------------------------------------------------ SU(N)
+template <int N, typename T> struct Mat { cx<T> e[N][N]; };
+
+template <int N, typename T> KLFT_HD Mat<N, T> mzero() {
+  Mat<N, T> m;
+#pragma unroll
+  for (int i = 0; i < N; ++i)
+#pragma unroll
+    for (int j = 0; j < N; ++j) m.e[i][j] = mk<T>(T(0), T(0));
+  return m;
+}
+template <int N, typename T> KLFT_HD Mat<N, T> mident() {
+  Mat<N, T> m = mzero<N, T>();
+#pragma unroll
+  for (int i = 0; i < N; ++i) m.e[i][i] = mk<T>(T(1), T(0));
+  return m;
+}
+// c = a * b (SUN.hpp:28-44 accumulation order)
+template <int N, typename T> KLFT_HD Mat<N, T> mul(const Mat<N, T> &a, const Mat<N, T> &b) {
+  Mat<N, T> c;
+#pragma unroll
+  for (int i = 0; i < N; ++i)
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+      cx<T> s = a.e[i][0] * b.e[0][j];
+#pragma unroll
+      for (int k = 1; k < N; ++k) s += a.e[i][k] * b.e[k][j];
+      c.e[i][j] = s;
+    }
+  return c;
+}
+// c = a * b^dagger
+template <int N, typename T> KLFT_HD Mat<N, T> mul_nd(const Mat<N, T> &a, const Mat<N, T> &b) {
+  Mat<N, T> c;
+#pragma unroll
+  for (int i = 0; i < N; ++i)
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+      cx<T> s = a.e[i][0] * conj(b.e[j][0]);
+#pragma unroll
+      for (int k = 1; k < N; ++k) s += a.e[i][k] * conj(b.e[j][k]);
+      c.e[i][j] = s;
+    }
+  return c;
+}
+// c = a^dagger * b^dagger
+template <int N, typename T> KLFT_HD Mat<N, T> mul_dd(const Mat<N, T> &a, const Mat<N, T> &b) {
+  Mat<N, T> c;
+#pragma unroll
+  for (int i = 0; i < N; ++i)
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+      cx<T> s = conj(a.e[0][i]) * conj(b.e[j][0]);
+#pragma unroll
+      for (int k = 1; k < N; ++k) s += conj(a.e[k][i]) * conj(b.e[j][k]);
+      c.e[i][j] = s;
+    }
+  return c;
+}
+// c = a^dagger * b
+template <int N, typename T> KLFT_HD Mat<N, T> mul_dn(const Mat<N, T> &a, const Mat<N, T> &b) {
+  Mat<N, T> c;
+#pragma unroll
+  for (int i = 0; i < N; ++i)
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+      cx<T> s = conj(a.e[0][i]) * b.e[0][j];
+#pragma unroll
+      for (int k = 1; k < N; ++k) s += conj(a.e[k][i]) * b.e[k][j];
+      c.e[i][j] = s;
+    }
+  return c;
+}
+template <int N, typename T> KLFT_HD Mat<N, T> dagger(const Mat<N, T> &a) {
+  Mat<N, T> c;
+#pragma unroll
+  for (int i = 0; i < N; ++i)
+#pragma unroll
+    for (int j = 0; j < N; ++j) c.e[i][j] = conj(a.e[j][i]);
+  return c;
+}
+template <int N, typename T> KLFT_HD void madd(Mat<N, T> &a, const Mat<N, T> &b) {
+#pragma unroll
+  for (int i = 0; i < N; ++i)
+#pragma unroll
+    for (int j = 0; j < N; ++j) a.e[i][j] += b.e[i][j];
+}
+template <int N, typename T> KLFT_HD Mat<N, T> mscale(const Mat<N, T> &a, T s) {
+  Mat<N, T> c;
+#pragma unroll
+  for (int i = 0; i < N; ++i)
+#pragma unroll
+    for (int j = 0; j < N; ++j) c.e[i][j] = a.e[i][j] * s;
+  return c;
+}
+// Re Tr(a * b) accumulated over the diagonal as Tr does (SUN.hpp:148-157)
+template <int N, typename T> KLFT_HD T retr_mul(const Mat<N, T> &a, const Mat<N, T> &b) {
+  T t = T(0);
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    cx<T> s = a.e[i][0] * b.e[0][i];
+#pragma unroll
+    for (int k = 1; k < N; ++k) s += a.e[i][k] * b.e[k][i];
+    t += s.re;
+  }
+  return t;
+}
+// sum_{ij} Re(a_ij * conj(b_ij)) = Re Tr(a b^dagger)  (GaugePlaquette.hpp:72-79)
+template <int N, typename T, typename A> KLFT_HD A retr_nd(const Mat<N, T> &a, const Mat<N, T> &b) {
+  A t = A(0);
+#pragma unroll
+  for (int i = 0; i < N; ++i)
+#pragma unroll
+    for (int j = 0; j < N; ++j) t += (A)a.e[i][j].re * (A)b.e[i][j].re + (A)a.e[i][j].im * (A)b.e[i][j].im;
+  return t;
+}
+
+// restoreSUN (SUN.hpp:256-340)
+template <typename T> KLFT_HD Mat<1, T> restore(const Mat<1, T> &a) {
+  Mat<1, T> c;
+  const T n = sqrt(a.e[0][0].re * a.e[0][0].re + a.e[0][0].im * a.e[0][0].im);
+  c.e[0][0] = cdiv(a.e[0][0], n);
+  return c;
+}
+template <typename T> KLFT_HD Mat<2, T> restore(const Mat<2, T> &a) {
+  Mat<2, T> c;
+  const T n = sqrt(a.e[0][0].re * a.e[0][0].re + a.e[0][0].im * a.e[0][0].im + a.e[0][1].re * a.e[0][1].re +
+                   a.e[0][1].im * a.e[0][1].im);
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 2; ++j) c.e[i][j] = cdiv(a.e[i][j], n);
+  return c;
+}
+template <typename T> KLFT_HD Mat<3, T> restore(const Mat<3, T> &a) {
+  Mat<3, T> c;
+  const T n0 = sqrt((conj(a.e[0][0]) * a.e[0][0] + conj(a.e[0][1]) * a.e[0][1] + conj(a.e[0][2]) * a.e[0][2]).re);
+  const T n1 = sqrt((conj(a.e[1][0]) * a.e[1][0] + conj(a.e[1][1]) * a.e[1][1] + conj(a.e[1][2]) * a.e[1][2]).re);
+#pragma unroll
+  for (int j = 0; j < 3; ++j) { c.e[0][j] = cdiv(a.e[0][j], n0); c.e[1][j] = cdiv(a.e[1][j], n1); }
+  c.e[2][0] = conj(c.e[0][1] * c.e[1][2] - c.e[0][2] * c.e[1][1]);
+  c.e[2][1] = conj(c.e[0][2] * c.e[1][0] - c.e[0][0] * c.e[1][2]);
+  c.e[2][2] = conj(c.e[0][0] * c.e[1][1] - c.e[0][1] * c.e[1][0]);
+  c.e[1][0] = conj(c.e[2][1] * c.e[0][2] - c.e[2][2] * c.e[0][1]);
+  c.e[1][1] = conj(c.e[2][2] * c.e[0][0] - c.e[2][0] * c.e[0][2]);
+  c.e[1][2] = conj(c.e[2][0] * c.e[0][1] - c.e[2][1] * c.e[0][0]);
+  return c;
+}
+
+// ------------------------------------------------------------------ geometry
+struct Geom {
+  int nd;
+  int L[4];      // extents (1 beyond nd)
+  int H[4];      // half extents
+  int hs[4];     // hidx strides
+  long long V, Vh;
+};
+
+// A site held as parity bits + half coordinates.
+struct Site {
+  int b[4];
+  int h[4];
+};
+
+KLFT_HD long long site_lin(const Geom &g, const Site &s) {
+  int sub = 0;
+  long long hidx = 0;
+#pragma unroll
+  for (int d = 0; d < 4; ++d) {
+    sub |= s.b[d] << d;
+    hidx += (long long)s.h[d] * g.hs[d];
+  }
+  return (long long)sub * g.Vh + hidx;
+}
+// lexicographic site index, x0 fastest (random-stream key and host layout)
+KLFT_HD uint32_t site_lex(const Geom &g, const Site &s) {
+  uint32_t lex = 0;
+#pragma unroll
+  for (int d = 3; d >= 0; --d) lex = lex * (uint32_t)g.L[d] + (uint32_t)(2 * s.h[d] + s.b[d]);
+  return lex;
+}
+// x + e_d (periodic)
+KLFT_HD Site site_up(const Geom &g, Site s, int d) {
+  if (s.b[d] == 0) {
+    s.b[d] = 1;
+  } else {
+    s.b[d] = 0;
+    s.h[d] = (s.h[d] + 1 == g.H[d]) ? 0 : s.h[d] + 1;
+  }
+  return s;
+}
+// x - e_d (periodic)
+KLFT_HD Site site_dn(const Geom &g, Site s, int d) {
+  if (s.b[d] == 1) {
+    s.b[d] = 0;
+  } else {
+    s.b[d] = 1;
+    s.h[d] = (s.h[d] == 0) ? g.H[d] - 1 : s.h[d] - 1;
+  }
+  return s;
+}
+// x + k e_d, any k >= 0 (periodic)
+KLFT_HD Site site_shift(const Geom &g, Site s, int d, int k) {
+  int x = 2 * s.h[d] + s.b[d];
+  x = (x + k) % g.L[d];
+  s.b[d] = x & 1;
+  s.h[d] = x >> 1;
+  return s;
+}
+KLFT_HD Site site_from_lin(const Geom &g, long long lin) {
+  Site s;
+  const int sub = (int)(lin / g.Vh);
+  long long hidx = lin - (long long)sub * g.Vh;
+#pragma unroll
+  for (int d = 0; d < 4; ++d) {
+    s.b[d] = (sub >> d) & 1;
+    s.h[d] = (int)(hidx % g.H[d]);
+    hidx /= g.H[d];
+  }
+  return s;
+}
+KLFT_HD Site site_from_lex(const Geom &g, long long lex) {
+  Site s;
+#pragma unroll
+  for (int d = 0; d < 4; ++d) {
+    const int x = (int)(lex % g.L[d]);
+    lex /= g.L[d];
+    s.b[d] = x & 1;
+    s.h[d] = x >> 1;
+  }
+  return s;
+}
+
+// ------------------------------------------------------------------ link field view
+template <int N, typename T> struct Links {
+  cx<T> *p;
+  long long V;
+  KLFT_D Mat<N, T> load(long long lin, int mu) const {
+    Mat<N, T> m;
+    const cx<T> *q = p + (long long)mu * N * N * V + lin;
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+#pragma unroll
+      for (int j = 0; j < N; ++j) m.e[i][j] = q[(i * N + j) * V];
+    return m;
+  }
+  KLFT_D void store(long long lin, int mu, const Mat<N, T> &m) const {
+    cx<T> *q = p + (long long)mu * N * N * V + lin;
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+#pragma unroll
+      for (int j = 0; j < N; ++j) q[(i * N + j) * V] = m.e[i][j];
+  }
+};
+
+// PTBC boundary defect (PTBCGaugeField.hpp:30-36, :187-198): links mu = 0 at
+// x0 = 0 whose x_1..x_{Nd-1} lie in pos + [0, len) (periodic) carry factor c.
+struct Defect {
+  int active;
+  int len;
+  int pos[3];
+  double c;
+};
+KLFT_HD bool in_defect(const Geom &g, const Defect &df, const Site &s, int mu) {
+  if (!df.active || mu != 0) return false;
+  if (2 * s.h[0] + s.b[0] != 0) return false;
+  for (int d = 1; d < g.nd; ++d) {
+    int rel = (2 * s.h[d] + s.b[d]) - df.pos[d - 1];
+    rel %= g.L[d];
+    if (rel < 0) rel += g.L[d];
+    if (rel >= df.len) return false;
+  }
+  return true;
+}
+
+// ------------------------------------------------------------------ reductions
+template <typename A> KLFT_D A warp_sum(A v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+}  // namespace klft

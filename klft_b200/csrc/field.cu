@@ -1,0 +1,211 @@
+// field.cu -- link-field utility kernels: cold/hot start, conversion between the
+// host interchange layout (AoS FP64, x0 fastest) and the device layout,
+// reunitarisation, the unitarity monitor and the all-links staple field.
+#include "group.cuh"
+#include "kernels.cuh"
+#include "staple.cuh"
+
+namespace klft {
+
+// deviceGaugeField init ctors (GaugeField.hpp:65-141): cold = identity
+// (lib/Metropolis.cpp:79-81); hot = Haar-random link from the (site, mu) stream.
+template <int NC, typename T>
+__global__ void init_kernel(Links<NC, T> U, Geom g, int hot, uint64_t seed, uint64_t chain) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= g.V * g.nd) return;
+  const long long lex = t / g.nd;
+  const int mu = (int)(t - lex * g.nd);
+  const Site s = site_from_lex(g, lex);
+  Mat<NC, T> m = mident<NC, T>();
+  if (hot) {
+    Stream st(seed, chain, (uint32_t)lex, 0u, KIND_INIT, (uint32_t)mu);
+    m = haar<T>(st, (const Mat<NC, T> *)nullptr);
+  }
+  U.store(site_lin(g, s), mu, m);
+}
+
+template <int NC, typename T>
+__global__ void import_kernel(Links<NC, T> U, Geom g, const double *__restrict__ aos) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= g.V * g.nd) return;
+  const long long lex = t / g.nd;
+  const int mu = (int)(t - lex * g.nd);
+  const double *p = aos + t * (2 * NC * NC);
+  Mat<NC, T> m;
+#pragma unroll
+  for (int i = 0; i < NC; ++i)
+#pragma unroll
+    for (int j = 0; j < NC; ++j) m.e[i][j] = mk<T>((T)p[2 * (i * NC + j)], (T)p[2 * (i * NC + j) + 1]);
+  U.store(site_lin(g, site_from_lex(g, lex)), mu, m);
+}
+
+template <int NC, typename T>
+__global__ void export_kernel(Links<NC, T> U, Geom g, double *__restrict__ aos) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= g.V * g.nd) return;
+  const long long lex = t / g.nd;
+  const int mu = (int)(t - lex * g.nd);
+  const Mat<NC, T> m = U.load(site_lin(g, site_from_lex(g, lex)), mu);
+  double *p = aos + t * (2 * NC * NC);
+#pragma unroll
+  for (int i = 0; i < NC; ++i)
+#pragma unroll
+    for (int j = 0; j < NC; ++j) {
+      p[2 * (i * NC + j)] = (double)m.e[i][j].re;
+      p[2 * (i * NC + j) + 1] = (double)m.e[i][j].im;
+    }
+}
+
+// restoreSUN on every link; the mixed form reunitarises in FP64
+template <int NC, typename T>
+__global__ void reunitarize_kernel(Links<NC, T> U, Geom g) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= g.V * g.nd) return;
+  const int mu = (int)(t / g.V);
+  const long long lin = t - (long long)mu * g.V;
+  const Mat<NC, T> m = U.load(lin, mu);
+  Mat<NC, double> d;
+#pragma unroll
+  for (int i = 0; i < NC; ++i)
+#pragma unroll
+    for (int j = 0; j < NC; ++j) d.e[i][j] = mk<double>((double)m.e[i][j].re, (double)m.e[i][j].im);
+  d = restore(d);
+  Mat<NC, T> o;
+#pragma unroll
+  for (int i = 0; i < NC; ++i)
+#pragma unroll
+    for (int j = 0; j < NC; ++j) o.e[i][j] = mk<T>((T)d.e[i][j].re, (T)d.e[i][j].im);
+  U.store(lin, mu, o);
+}
+
+template <int NC, typename T>
+__global__ void unitarity_kernel(Links<NC, T> U, Geom g, double *part) {
+  double worst = 0.0;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < g.V * g.nd;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int mu = (int)(t / g.V);
+    const long long lin = t - (long long)mu * g.V;
+    const Mat<NC, T> m = U.load(lin, mu);
+    Mat<NC, double> d;
+#pragma unroll
+    for (int i = 0; i < NC; ++i)
+#pragma unroll
+      for (int j = 0; j < NC; ++j) d.e[i][j] = mk<double>((double)m.e[i][j].re, (double)m.e[i][j].im);
+    const Mat<NC, double> p = mul_dn(d, d);
+    double e = 0.0;
+#pragma unroll
+    for (int i = 0; i < NC; ++i)
+#pragma unroll
+      for (int j = 0; j < NC; ++j) {
+        const double re = p.e[i][j].re - (i == j ? 1.0 : 0.0), im = p.e[i][j].im;
+        e += re * re + im * im;
+      }
+    worst = fmax(worst, sqrt(e));
+  }
+  __shared__ double red[256];
+  red[threadIdx.x] = worst;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + s]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+}
+
+__global__ void max_partials_kernel(const double *part, int n, double *out) {
+  __shared__ double red[256];
+  double w = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) w = fmax(w, part[i]);
+  red[threadIdx.x] = w;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + s]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = red[0];
+}
+
+// Gauge_Util.hpp:27-97 stapleField: the staple of every (x, mu), in host layout
+template <int NC, int ND, typename T>
+__global__ void staple_field_kernel(Links<NC, T> U, Geom g, double *__restrict__ aos) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= g.V * ND) return;
+  const long long lex = t / ND;
+  const int mu = (int)(t - lex * ND);
+  const Site x = site_from_lex(g, lex);
+  Defect none{0, 1, {0, 0, 0}, 1.0};
+  const Mat<NC, T> S = staple<NC, ND, T>(U, g, x, mu, none);
+  double *p = aos + t * (2 * NC * NC);
+#pragma unroll
+  for (int i = 0; i < NC; ++i)
+#pragma unroll
+    for (int j = 0; j < NC; ++j) {
+      p[2 * (i * NC + j)] = (double)S.e[i][j].re;
+      p[2 * (i * NC + j) + 1] = (double)S.e[i][j].im;
+    }
+}
+
+#define KLFT_DISPATCH_NC_T(nc, dtype, CALL)                        \
+  do {                                                            \
+    if (dtype == 0) {                                             \
+      if (nc == 1) { using T = double; constexpr int NC = 1; CALL; } \
+      else if (nc == 2) { using T = double; constexpr int NC = 2; CALL; } \
+      else if (nc == 3) { using T = double; constexpr int NC = 3; CALL; } \
+      else return cudaErrorInvalidValue;                          \
+    } else {                                                      \
+      if (nc == 1) { using T = float; constexpr int NC = 1; CALL; } \
+      else if (nc == 2) { using T = float; constexpr int NC = 2; CALL; } \
+      else if (nc == 3) { using T = float; constexpr int NC = 3; CALL; } \
+      else return cudaErrorInvalidValue;                          \
+    }                                                             \
+  } while (0)
+
+static inline unsigned nblocks(long long n, int b) { return (unsigned)((n + b - 1) / b); }
+
+cudaError_t launch_init(int nc, int dtype, void *links, const Geom &g, int hot, uint64_t seed, uint64_t chain,
+                        cudaStream_t st) {
+  KLFT_DISPATCH_NC_T(nc, dtype, (init_kernel<NC, T><<<nblocks(g.V * g.nd, 256), 256, 0, st>>>(
+                                    Links<NC, T>{(cx<T> *)links, g.V}, g, hot, seed, chain)));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_import(int nc, int dtype, void *links, const Geom &g, const double *aos, cudaStream_t st) {
+  KLFT_DISPATCH_NC_T(nc, dtype, (import_kernel<NC, T><<<nblocks(g.V * g.nd, 256), 256, 0, st>>>(
+                                    Links<NC, T>{(cx<T> *)links, g.V}, g, aos)));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_export(int nc, int dtype, const void *links, const Geom &g, double *aos, cudaStream_t st) {
+  KLFT_DISPATCH_NC_T(nc, dtype, (export_kernel<NC, T><<<nblocks(g.V * g.nd, 256), 256, 0, st>>>(
+                                    Links<NC, T>{(cx<T> *)links, g.V}, g, aos)));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_reunitarize(int nc, int dtype, void *links, const Geom &g, cudaStream_t st) {
+  KLFT_DISPATCH_NC_T(nc, dtype, (reunitarize_kernel<NC, T><<<nblocks(g.V * g.nd, 256), 256, 0, st>>>(
+                                    Links<NC, T>{(cx<T> *)links, g.V}, g)));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_unitarity(int nc, int dtype, const void *links, const Geom &g, double *d_part, double *d_out,
+                             cudaStream_t st) {
+  const int nb = 296;
+  KLFT_DISPATCH_NC_T(nc, dtype, (unitarity_kernel<NC, T><<<nb, 256, 0, st>>>(
+                                    Links<NC, T>{(cx<T> *)links, g.V}, g, d_part)));
+  max_partials_kernel<<<1, 256, 0, st>>>(d_part, nb, d_out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_staple_field(int nc, int dtype, const void *links, const Geom &g, double *aos, cudaStream_t st) {
+  const unsigned nb = nblocks(g.V * g.nd, 128);
+#define KLFT_SF(NDV) staple_field_kernel<NC, NDV, T><<<nb, 128, 0, st>>>(Links<NC, T>{(cx<T> *)links, g.V}, g, aos)
+  KLFT_DISPATCH_NC_T(nc, dtype, ({
+    if (g.nd == 2) KLFT_SF(2);
+    else if (g.nd == 3) KLFT_SF(3);
+    else KLFT_SF(4);
+  }));
+#undef KLFT_SF
+  return cudaGetLastError();
+}
+
+}  // namespace klft

@@ -1,0 +1,45 @@
+// kernels.cuh -- host-side launch interface of the device kernels.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace klft {
+
+struct MetroArgs {
+  double beta, delta, eps;
+  int nhits, proposal;
+  uint64_t seed, chain;
+};
+
+// dtype: 0 = double (plain FP64 form), 1 = float (mixed form)
+cudaError_t launch_metropolis_pass(int nc, int dtype, void *links, const Geom &g, int val, const MetroArgs &a,
+                                   const uint32_t *d_sweep, unsigned long long *d_nacc, const Defect &df, int block,
+                                   cudaStream_t st);
+cudaError_t launch_advance(uint32_t *d_counter, cudaStream_t st);
+
+cudaError_t launch_init(int nc, int dtype, void *links, const Geom &g, int hot, uint64_t seed, uint64_t chain,
+                        cudaStream_t st);
+// host AoS FP64 staging buffer <-> device layout
+cudaError_t launch_import(int nc, int dtype, void *links, const Geom &g, const double *aos, cudaStream_t st);
+cudaError_t launch_export(int nc, int dtype, const void *links, const Geom &g, double *aos, cudaStream_t st);
+cudaError_t launch_reunitarize(int nc, int dtype, void *links, const Geom &g, cudaStream_t st);
+// max ||U^dagger U - 1||_F -> *d_out (via partials)
+cudaError_t launch_unitarity(int nc, int dtype, const void *links, const Geom &g, double *d_part, double *d_out,
+                             cudaStream_t st);
+// staples of every link, written in host AoS FP64 layout
+cudaError_t launch_staple_field(int nc, int dtype, const void *links, const Geom &g, double *aos, cudaStream_t st);
+
+// sum over sites of sum_{mu<nu} Re Tr P_{mu nu}, unnormalised, into *d_out
+cudaError_t launch_plaquette(int nc, int dtype, const void *links, const Geom &g, double *d_part, int nblk,
+                             double *d_out, cudaStream_t st);
+// Wilson loops of a pair list in the (mu, nu) plane; d_out[k] = sum over sites Re Tr W
+cudaError_t launch_wilson_direct(int nc, int dtype, const void *links, const Geom &g, int mu, int nu,
+                                 const int *d_pairs, int npairs, double *d_part, int nblk, double *d_out,
+                                 cudaStream_t st);
+
+int plaquette_blocks(const Geom &g);
+// ordered final reduction of nblk partials for each of n outputs
+cudaError_t launch_reduce_partials(const double *d_part, int nblk, int n, double *d_out, cudaStream_t st);
+
+}  // namespace klft
