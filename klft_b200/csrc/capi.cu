@@ -164,7 +164,8 @@ klft_status klft_lattice_destroy(klft_lattice *lat) {
   {
     LOCK(lat);
     if (lat->stream) cudaStreamSynchronize(lat->stream);
-    for (Scratch *s : {&lat->s_part, &lat->s_out, &lat->s_aux, &lat->s_stage, &lat->s_wl, &lat->s_hmc})
+    for (Scratch *s : {&lat->s_part, &lat->s_out, &lat->s_aux, &lat->s_stage, &lat->s_wl, &lat->s_hmc,
+                        &lat->s_gf, &lat->s_tab})
       s->release();
     if (lat->links) cudaFree(lat->links);
     if (lat->d_counters) cudaFree(lat->d_counters);
@@ -361,21 +362,21 @@ klft_status klft_run_cycles(klft_lattice *lat, double beta, double delta, int nh
   LOCK(lat);
   const int nd = lat->g.nd;
   const int nw = (nd - 1) * npairs;  // per cycle: one sum per (spatial mu, pair)
-  // aux layout: [pairs (2*npairs int, padded)] [nacc (ncycles u64)] ; out layout: [plaq ncycles][w ncycles*nw]
-  const size_t pair_bytes = ((size_t)npairs * 2 * sizeof(int) + 15) & ~(size_t)15;
-  CK(lat->s_aux.ensure(pair_bytes + (size_t)ncycles * sizeof(unsigned long long)));
+  // aux: nacc (ncycles u64); wl: [plaq ncycles][w ncycles*nw]; all scratch sized before the first launch
+  CK(lat->s_aux.ensure((size_t)ncycles * sizeof(unsigned long long)));
   CK(lat->s_wl.ensure((size_t)ncycles * (1 + nw) * sizeof(double)));
-  int *d_pairs = (int *)lat->s_aux.ptr;
-  unsigned long long *d_nacc = (unsigned long long *)((char *)lat->s_aux.ptr + pair_bytes);
+  unsigned long long *d_nacc = (unsigned long long *)lat->s_aux.ptr;
   double *d_plaq = (double *)lat->s_wl.ptr;
   double *d_w = d_plaq + ncycles;
-  if (npairs > 0)
-    CK(cudaMemcpyAsync(d_pairs, temporal_pairs, (size_t)npairs * 2 * sizeof(int), cudaMemcpyHostToDevice,
-                       lat->stream));
+  WilsonPlan plan;
+  if (npairs > 0) {
+    klft_status s = make_wilson_plan(lat, temporal_pairs, npairs, nd - 1, plan);
+    if (s != KLFT_OK) return s;
+  }
   CK(cudaMemsetAsync(d_nacc, 0, (size_t)ncycles * sizeof(unsigned long long), lat->stream));
   {
     const int nblk = plaquette_blocks(lat->g);
-    CK(lat->s_part.ensure((size_t)nblk * (npairs > 1 ? npairs : 1) * sizeof(double)));
+    if (lat->s_part.cap < (size_t)nblk * sizeof(double)) CK(lat->s_part.ensure((size_t)nblk * sizeof(double)));
   }
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
@@ -386,12 +387,12 @@ klft_status klft_run_cycles(klft_lattice *lat, double beta, double delta, int nh
     if (s != KLFT_OK) return s;
     if (measure_plaquette) {
       const int nblk = plaquette_blocks(lat->g);
-      CK(lat->s_part.ensure((size_t)nblk * sizeof(double)));
       CK(launch_plaquette(lat->nc, lat->dtype(), lat->links, lat->g, (double *)lat->s_part.ptr, nblk, d_plaq + c,
                           lat->stream));
     }
     for (int mu = 0; mu < nd - 1 && npairs > 0; ++mu) {
-      s = enqueue_wilson(lat, mu, nd - 1, d_pairs, npairs, d_w + (size_t)c * nw + (size_t)mu * npairs);
+      // the axial-gauge transformation along nu = Nd-1 is shared by the spatial planes
+      s = enqueue_wilson_plane(lat, plan, mu, nd - 1, mu > 0, d_w + (size_t)c * nw + (size_t)mu * npairs);
       if (s != KLFT_OK) return s;
     }
   }
@@ -470,21 +471,68 @@ double normalize_wilson(const klft_lattice *lat, double sum) {
   return w;
 }
 
-// enqueue: d_out[k] = unnormalised sum over sites of Re Tr W for pair k (device pairs)
-klft_status enqueue_wilson(klft_lattice *lat, int mu, int nu, const int *d_pairs, int npairs, double *d_out) {
-  const int nblk = plaquette_blocks(lat->g);
-  CK(lat->s_part.ensure((size_t)nblk * npairs * sizeof(double)));
-  CK(launch_wilson_direct(lat->nc, lat->dtype(), lat->links, lat->g, mu, nu, d_pairs, npairs,
-                          (double *)lat->s_part.ptr, nblk, d_out, lat->stream));
+// Build the device tables for a pair list: the pairs themselves (direct form)
+// and, for the gauge-fixed form, the (T, pair) lists per loop length L.  All
+// scratch the plane kernels need is sized here, before anything is enqueued.
+klft_status make_wilson_plan(klft_lattice *lat, const int *pairs, int npairs, int nu, WilsonPlan &plan) {
+  plan = WilsonPlan();
+  plan.npairs = npairs;
+  bool degenerate = false;
+  for (int k = 0; k < npairs; ++k) {
+    plan.lmax = pairs[2 * k] > plan.lmax ? pairs[2 * k] : plan.lmax;
+    plan.tmax = pairs[2 * k + 1] > plan.tmax ? pairs[2 * k + 1] : plan.tmax;
+    if (pairs[2 * k] == 0 || pairs[2 * k + 1] == 0) degenerate = true;
+  }
+  const size_t smem = wilson_gf_smem(lat->nc, lat->dtype(), lat->g, nu, plan.tmax, npairs);
+  plan.gf = !degenerate && npairs > 0 && smem <= 200 * 1024;
+  std::vector<int> h;
+  h.insert(h.end(), pairs, pairs + 2 * npairs);
+  if (plan.gf) {
+    std::vector<int> off(plan.lmax + 2, 0), tl, pl;
+    for (int L = 1; L <= plan.lmax; ++L) {
+      off[L] = (int)tl.size();
+      for (int k = 0; k < npairs; ++k)
+        if (pairs[2 * k] == L) { tl.push_back(pairs[2 * k + 1]); pl.push_back(k); }
+    }
+    off[plan.lmax + 1] = (int)tl.size();
+    off[0] = 0;
+    plan.off_at = (int)h.size(); h.insert(h.end(), off.begin(), off.end());
+    plan.t_at = (int)h.size(); h.insert(h.end(), tl.begin(), tl.end());
+    plan.p_at = (int)h.size(); h.insert(h.end(), pl.begin(), pl.end());
+    CK(lat->s_gf.ensure(wilson_gf_scratch(lat->nc, lat->dtype(), lat->g, nu, plan.tmax)));
+  }
+  CK(lat->s_tab.ensure(h.size() * sizeof(int) + 16));
+  CK(cudaMemcpyAsync(lat->s_tab.ptr, h.data(), h.size() * sizeof(int), cudaMemcpyHostToDevice, lat->stream));
+  CK(cudaStreamSynchronize(lat->stream));  // h is pageable and local
+  const int nblk = plan.gf ? wilson_gf_blocks(lat->g) : plaquette_blocks(lat->g);
+  CK(lat->s_part.ensure((size_t)nblk * (npairs > 1 ? npairs : 1) * sizeof(double)));
+  return KLFT_OK;
+}
+
+// enqueue: d_out[k] = unnormalised sum over sites of Re Tr W for pair k of the plan
+klft_status enqueue_wilson_plane(klft_lattice *lat, const WilsonPlan &plan, int mu, int nu, bool omega_ready,
+                                 double *d_out) {
+  const int *tab = (const int *)lat->s_tab.ptr;
+  if (plan.gf) {
+    const int *dt[3] = {tab + plan.off_at, tab + plan.t_at, tab + plan.p_at};
+    CK(launch_wilson_gf(lat->nc, lat->dtype(), lat->links, lat->g, mu, nu, dt, nullptr, plan.lmax, plan.tmax,
+                        plan.npairs, omega_ready, lat->s_gf.ptr, (double *)lat->s_part.ptr, wilson_gf_blocks(lat->g),
+                        d_out, lat->stream));
+  } else {
+    const int nblk = plaquette_blocks(lat->g);
+    CK(launch_wilson_direct(lat->nc, lat->dtype(), lat->links, lat->g, mu, nu, tab, plan.npairs,
+                            (double *)lat->s_part.ptr, nblk, d_out, lat->stream));
+  }
   return KLFT_OK;
 }
 
 // unnormalised sums over sites for a list of (Lmu, Lnu) pairs in the (mu, nu) plane
 klft_status wilson_sums(klft_lattice *lat, int mu, int nu, const int *pairs, int npairs, double *sums) {
   CK(lat->s_out.ensure((size_t)(npairs > KLFT_RESULT_SLOTS ? npairs : KLFT_RESULT_SLOTS) * sizeof(double)));
-  CK(lat->s_aux.ensure((size_t)npairs * 2 * sizeof(int)));
-  CK(cudaMemcpyAsync(lat->s_aux.ptr, pairs, (size_t)npairs * 2 * sizeof(int), cudaMemcpyHostToDevice, lat->stream));
-  klft_status s = enqueue_wilson(lat, mu, nu, (const int *)lat->s_aux.ptr, npairs, (double *)lat->s_out.ptr);
+  WilsonPlan plan;
+  klft_status s = make_wilson_plan(lat, pairs, npairs, nu, plan);
+  if (s != KLFT_OK) return s;
+  s = enqueue_wilson_plane(lat, plan, mu, nu, false, (double *)lat->s_out.ptr);
   if (s != KLFT_OK) return s;
   CK(cudaMemcpyAsync(sums, lat->s_out.ptr, (size_t)npairs * sizeof(double), cudaMemcpyDeviceToHost, lat->stream));
   CK(cudaStreamSynchronize(lat->stream));

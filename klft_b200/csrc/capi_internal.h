@@ -36,7 +36,7 @@ struct klft_lattice {
   cudaStream_t stream = nullptr;
   uint32_t *d_counters = nullptr;  // [0] sweep, [1] trajectory, [2] cycle
   double *h_results = nullptr;     // pinned, KLFT_RESULT_SLOTS doubles
-  klft::Scratch s_part, s_out, s_aux, s_stage, s_wl, s_hmc;
+  klft::Scratch s_part, s_out, s_aux, s_stage, s_wl, s_hmc, s_gf, s_tab;
   klft::Defect defect{0, 1, {0, 0, 0}, 1.0};
   std::mutex mtx;
   int dtype() const { return precision == KLFT_PRECISION_FP64 ? 0 : 1; }
@@ -49,6 +49,14 @@ klft_status enqueue_sweeps(klft_lattice *lat, double beta, double delta, int nhi
 klft_status enqueue_plaquette(klft_lattice *lat, int slot);
 double normalize_plaquette(const klft_lattice *lat, double sum);
 double normalize_wilson(const klft_lattice *lat, double sum);
-klft_status enqueue_wilson(klft_lattice *lat, int mu, int nu, const int *d_pairs, int npairs, double *d_out);
+// Device tables of a Wilson-loop pair list (offsets are int indices into s_tab).
+struct WilsonPlan {
+  int npairs = 0, lmax = 0, tmax = 0;
+  bool gf = false;
+  int off_at = 0, t_at = 0, p_at = 0;
+};
+klft_status make_wilson_plan(klft_lattice *lat, const int *pairs, int npairs, int nu, WilsonPlan &plan);
+klft_status enqueue_wilson_plane(klft_lattice *lat, const WilsonPlan &plan, int mu, int nu, bool omega_ready,
+                                 double *d_out);
 klft_status wilson_sums(klft_lattice *lat, int mu, int nu, const int *pairs, int npairs, double *sums);
 }  // namespace klft

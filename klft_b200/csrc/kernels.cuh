@@ -38,6 +38,15 @@ cudaError_t launch_wilson_direct(int nc, int dtype, const void *links, const Geo
                                  const int *d_pairs, int npairs, double *d_part, int nblk, double *d_out,
                                  cudaStream_t st);
 
+// Wilson loops of a pair list in the (mu, nu) plane by axial gauge fixing (wilson.cu)
+size_t wilson_gf_scratch(int nc, int dtype, const Geom &g, int nu, int tmax);
+size_t wilson_gf_smem(int nc, int dtype, const Geom &g, int nu, int tmax, int npairs);
+int wilson_gf_blocks(const Geom &g);
+cudaError_t launch_wilson_gf(int nc, int dtype, const void *links, const Geom &g, int mu, int nu,
+                             const int *const *d_tab, const int *h_off, int lmax, int tmax, int npairs,
+                             bool omega_ready, void *scratch, double *d_part, int nblk, double *d_out,
+                             cudaStream_t st);
+
 int plaquette_blocks(const Geom &g);
 // ordered final reduction of nblk partials for each of n outputs
 cudaError_t launch_reduce_partials(const double *d_part, int nblk, int n, double *d_out, cudaStream_t st);

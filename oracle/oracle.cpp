@@ -234,20 +234,54 @@ static inline void randsun(Mat<2> &r, Stream &g, double delta, int, double) {
   r.a[1][0] = cplx(-r.a[0][1].real(), r.a[0][1].imag());
   r.a[1][1] = cplx(r.a[0][0].real(), -r.a[0][0].imag());
 }
-// SUN.hpp:192-251 (reference proposal) or X = exp(i eps H), H = sum_a h_a lambda_a/2,
-// h_a ~ N(0,1) from four Box-Muller pairs (project proposal for SU(3)).
-static inline void randsun(Mat<3> &r, Stream &g, double delta, int proposal, double eps) {
-  if (proposal == PROPOSAL_EXP) {
-    double h[8];
-    for (int k = 0; k < 4; ++k) g.gauss2(h[2 * k], h[2 * k + 1]);
-    Mat<3> H = zero<3>();
-    for (int a = 0; a < 8; ++a) {
-      Mat<3> l = gellmann(a);
-      for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) H.a[i][j] += (0.5 * eps * h[a]) * l.a[i][j];
-    }
-    r = expi_herm3(H);
-    return;
+// Project SU(3) proposal X = exp(i eps H), H = sum_a h_a lambda_a / 2, h_a ~ N(0,1).
+// It has no counterpart in the reference, so its random numbers sit at fixed
+// positions of the (sweep, site) stream: hit h of the site (h = mu*nHits + hit)
+// takes Philox blocks 3h and 3h+1 for eight 32-bit uniforms u = (w + 1/2) 2^-32
+// (Box-Muller pairs (u0,u1), (u2,u3), (u4,u5), (u6,u7)) and block 3h+2 for the
+// 53-bit accept uniform.  A proposal therefore does not depend on earlier accept
+// decisions.
+struct ExpHit {
+  uint32_t key[2], site, step;
+  ExpHit(uint64_t seed, uint64_t chain, uint32_t site_, uint32_t step_) : site(site_), step(step_) {
+    key[0] = (uint32_t)seed;
+    key[1] = (uint32_t)(seed >> 32) ^ (uint32_t)chain;
   }
+  void block(uint32_t b, uint32_t out[4]) const {
+    uint32_t ctr[4] = {b, site, step, KIND_METROPOLIS << 24};
+    philox(ctr, key, out);
+  }
+  void gauss8(uint32_t h, double g[8]) const {
+    uint32_t w[8];
+    block(3 * h, w);
+    block(3 * h + 1, w + 4);
+    for (int k = 0; k < 4; ++k) {
+      const double ua = ((double)w[2 * k] + 0.5) * 0x1.0p-32, ub = ((double)w[2 * k + 1] + 0.5) * 0x1.0p-32;
+      const double r = std::sqrt(-2.0 * std::log(ua));
+      g[2 * k] = r * std::cos(6.283185307179586 * ub);
+      g[2 * k + 1] = r * std::sin(6.283185307179586 * ub);
+    }
+  }
+  double accept_uniform(uint32_t h) const {
+    uint32_t w[4];
+    block(3 * h + 2, w);
+    return (double)((((uint64_t)w[0] << 32) | w[1]) >> 11) * 0x1.0p-53;
+  }
+};
+
+static Mat<3> exp_proposal(const ExpHit &eh, uint32_t h, double eps) {
+  double hh[8];
+  eh.gauss8(h, hh);
+  Mat<3> H = zero<3>();
+  for (int a = 0; a < 8; ++a) {
+    Mat<3> l = gellmann(a);
+    for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) H.a[i][j] += (0.5 * eps * hh[a]) * l.a[i][j];
+  }
+  return expi_herm3(H);
+}
+
+// SUN.hpp:192-251: reference Gram-Schmidt proposal
+static inline void randsun(Mat<3> &r, Stream &g, double delta, int, double) {
   double r1[6], r2[6], norm, fact;
   cplx z1[3], z2[3], z3[3], z;
   while (true) {
@@ -437,18 +471,26 @@ static double metropolis_sweep(const Field<NC> &F, double beta, double delta, in
       for (int d = 0; d < nd; ++d) { x[d] = 2 * (int)(t % H[d]) + bit[d]; t /= H[d]; }  // IndexHelper.hpp:68-81
       long s = g.lex(x);
       Stream rng(seed, chain, (uint32_t)s, sweep, KIND_METROPOLIS, 0);
+      const ExpHit eh(seed, chain, (uint32_t)s, sweep);
+      const bool expprop = NC == 3 && proposal == PROPOSAL_EXP;
       for (int mu = 0; mu < nd; ++mu) {
         const Mat<NC> S = staple(F, s, mu);
         const double c = link_factor(g, F.df, s, mu);
         for (int hit = 0; hit < nHits; ++hit) {
+          const uint32_t h = (uint32_t)(mu * nHits + hit);
           Mat<NC> r;
-          randsun(r, rng, delta, proposal, eps);
+          if constexpr (NC == 3) {
+            if (expprop) r = exp_proposal(eh, h, eps);
+            else randsun(r, rng, delta, proposal, eps);
+          } else {
+            randsun(r, rng, delta, proposal, eps);
+          }
           const Mat<NC> Uold = F.raw(s, mu);
           const Mat<NC> Unew = mul(Uold, r);
           double dS = -(beta / (double)NC) * (trace(mul(Unew, S)).real() - trace(mul(Uold, S)).real());
           if (c != 1.0) dS *= c;
           bool accept = dS < 0.0;
-          if (!accept) accept = (rng.drand(0.0, 1.0) < std::exp(-dS));
+          if (!accept) accept = ((expprop ? eh.accept_uniform(h) : rng.drand(0.0, 1.0)) < std::exp(-dS));
           if (accept) {
             F.put(s, mu, restore(Unew));
             ++nacc;

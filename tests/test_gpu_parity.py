@@ -150,3 +150,41 @@ def test_invalid_arguments_raise():
     with pytest.raises(klft_b200.KlftError):
         g.metropolis(1.0, 0.1, 1, 1, proposal="exp", eps=0.1) if False else g.wilson_loop_temporal([(-1, 2)])
     g.close()
+
+
+@pytest.mark.parametrize("precision,rtol,atol", [("fp64", 1e-12, 1e-14), ("mixed", 0.0, 2e-6)])
+def test_wilson_loops_longer_than_lattice(oracle, precision, rtol, atol):
+    """Gauge-fixed loops that wrap the lattice once or twice in either direction."""
+    lat = Lat(3, [4, 6, 4, 6])
+    U = oracle.init(lat, True, 17)
+    g = gf(lat.L, 3, precision)
+    g.upload(U)
+    pairs = [(1, 1), (4, 3), (5, 6), (7, 13), (2, 12), (9, 1)]
+    np.testing.assert_allclose(g.wilson_loop_temporal(pairs), oracle.wilson_temporal(lat, U, pairs), rtol=rtol,
+                               atol=atol)
+    for mu, nu in [(3, 0), (1, 2), (0, 3)]:
+        np.testing.assert_allclose(g.wilson_loop_mu_nu(mu, nu, pairs), oracle.wilson_mu_nu(lat, U, mu, nu, pairs),
+                                   rtol=rtol, atol=atol)
+
+
+@pytest.mark.parametrize("L", [[6, 4, 4, 12], [4, 4, 20], [10, 6]])
+def test_wilson_loops_uneven_extents(oracle, L):
+    """Temporal extents that do not divide the warp (columns straddle warps)."""
+    lat = Lat(2, L)
+    U = oracle.init(lat, True, 23)
+    g = gf(L, 2)
+    g.upload(U)
+    pairs = [(l, t) for l in range(1, 5) for t in range(1, 6)]
+    np.testing.assert_allclose(g.wilson_loop_temporal(pairs), oracle.wilson_temporal(lat, U, pairs), rtol=1e-12,
+                               atol=1e-14)
+
+
+def test_wilson_degenerate_pairs(oracle):
+    """Zero-extent loops (routed to the direct kernel) equal 1 up to round-off."""
+    lat = Lat(3, [4, 4, 4, 4])
+    U = oracle.init(lat, True, 29)
+    g = gf(lat.L, 3)
+    g.upload(U)
+    pairs = [(0, 2), (2, 0), (0, 0), (2, 2)]
+    np.testing.assert_allclose(g.wilson_loop_temporal(pairs), oracle.wilson_temporal(lat, U, pairs), rtol=1e-12,
+                               atol=1e-14)
