@@ -14,11 +14,45 @@ enum Proposal : int { PROPOSAL_REFERENCE = 0, PROPOSAL_EXP = 1 };
 // exp(iQ) for hermitian traceless 3x3 Q by the Cayley-Hamilton form of
 // Morningstar & Peardon, Phys. Rev. D 69 (2004) 054501, eqs. (23)-(34):
 // exp(iQ) = f0 + f1 Q + f2 Q^2 with the f_j from c0 = det Q, c1 = Tr Q^2 / 2.
+// Q^2 of a hermitian Q: the upper triangle, mirrored.
+template <typename T> KLFT_D Mat<3, T> herm_square(const Mat<3, T> &Q) {
+  Mat<3, T> Q2;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    T d = T(0);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) d += Q.e[i][k].re * Q.e[i][k].re + Q.e[i][k].im * Q.e[i][k].im;
+    Q2.e[i][i] = mk<T>(d, T(0));
+#pragma unroll
+    for (int j = i + 1; j < 3; ++j) {
+      cx<T> s = Q.e[i][0] * Q.e[0][j];
+#pragma unroll
+      for (int k = 1; k < 3; ++k) s += Q.e[i][k] * Q.e[k][j];
+      Q2.e[i][j] = s;
+      Q2.e[j][i] = conj(s);
+    }
+  }
+  return Q2;
+}
+
+// Fast single-precision functions for the mixed form.  The arguments of the
+// SU(3) exponential are bounded (|x| <= pi), where the SFU forms are accurate
+// to about 1e-6 absolute, the round-off level of FP32 links.
+struct FastMath {
+  static KLFT_D float fsin(float x) { return __sinf(x); }
+  static KLFT_D float fcos(float x) { return __cosf(x); }
+  static KLFT_D double fsin(double x) { return sin(x); }
+  static KLFT_D double fcos(double x) { return cos(x); }
+};
+
 template <typename T> KLFT_D Mat<3, T> expi_su3(const Mat<3, T> &Q) {
-  const Mat<3, T> Q2 = mul(Q, Q);
+  const Mat<3, T> Q2 = herm_square(Q);
   const T c1 = T(0.5) * (Q2.e[0][0].re + Q2.e[1][1].re + Q2.e[2][2].re);
-  // c0 = det Q = Tr(Q^3)/3 = Re Tr(Q Q^2)/3 for hermitian Q
-  const T c0 = retr_mul(Q, Q2) / T(3);
+  // c0 = det Q, real for hermitian Q
+  const T c0 = Q.e[0][0].re * (Q.e[1][1].re * Q.e[2][2].re - (Q.e[1][2].re * Q.e[1][2].re + Q.e[1][2].im * Q.e[1][2].im)) -
+               Q.e[1][1].re * (Q.e[0][2].re * Q.e[0][2].re + Q.e[0][2].im * Q.e[0][2].im) -
+               Q.e[2][2].re * (Q.e[0][1].re * Q.e[0][1].re + Q.e[0][1].im * Q.e[0][1].im) +
+               T(2) * (Q.e[0][1] * Q.e[1][2] * Q.e[2][0]).re;
   cx<T> f0, f1, f2;
   const T tiny = sizeof(T) == 8 ? T(1e-16) : T(1e-10);
   if (c1 < tiny) {
@@ -33,19 +67,18 @@ template <typename T> KLFT_D Mat<3, T> expi_su3(const Mat<3, T> &Q) {
     T ratio = ac0 / c0max;
     ratio = ratio > T(1) ? T(1) : ratio;
     const T theta = acos(ratio);
-    const T u = sqrt(c1 / T(3)) * cos(theta / T(3));
-    const T w = sqrt(c1) * sin(theta / T(3));
+    const T u = sqrt(c1 / T(3)) * FastMath::fcos(theta / T(3));
+    const T w = sqrt(c1) * FastMath::fsin(theta / T(3));
     const T u2 = u * u, w2 = w * w;
     T xi0;
     if (fabs(w) < T(0.05)) {
       xi0 = T(1) - w2 / T(6) * (T(1) - w2 / T(20) * (T(1) - w2 / T(42)));
     } else {
-      xi0 = sin(w) / w;
+      xi0 = FastMath::fsin(w) / w;
     }
-    const T cw = cos(w);
-    T s2u, c2u, smu, cmu;
-    s2u = sin(T(2) * u); c2u = cos(T(2) * u);
-    smu = sin(-u); cmu = cos(-u);
+    const T cw = FastMath::fcos(w);
+    const T s2u = FastMath::fsin(T(2) * u), c2u = FastMath::fcos(T(2) * u);
+    const T smu = -FastMath::fsin(u), cmu = FastMath::fcos(u);
     const cx<T> e2iu = mk<T>(c2u, s2u);
     const cx<T> emiu = mk<T>(cmu, smu);
     const cx<T> h0 = e2iu * (u2 - w2) + emiu * mk<T>(T(8) * u2 * cw, T(2) * u * (T(3) * u2 + w2) * xi0);

@@ -51,13 +51,15 @@ KLFT_D void box_muller(uint32_t wa, uint32_t wb, double &g0, double &g1) {
   g0 = r * c;
   g1 = r * s;
 }
+// Mixed form: SFU log and sincos.  cos/sin(2 pi u) = -cos/sin(2 pi (u - 1/2)) keeps
+// the SFU argument in [-pi, pi].
 KLFT_D void box_muller(uint32_t wa, uint32_t wb, float &g0, float &g1) {
   const float ua = fmaf((float)wa, 0x1.0p-32f, 0x1.0p-33f), ub = fmaf((float)wb, 0x1.0p-32f, 0x1.0p-33f);
-  const float r = sqrtf(-2.0f * logf(ua));
+  const float r = sqrtf(-2.0f * __logf(ua));
   float s, c;
-  sincospif(2.0f * ub, &s, &c);
-  g0 = r * c;
-  g1 = r * s;
+  __sincosf(6.28318530717958648f * (ub - 0.5f), &s, &c);
+  g0 = -r * c;
+  g1 = -r * s;
 }
 
 template <typename T>
