@@ -30,17 +30,47 @@ KLFT_D double block_sum(double v) {
   return s;
 }
 
-template <int NC, int ND, typename T>
-__global__ void __launch_bounds__(RED_THREADS) plaquette_kernel(Links<NC, T> U, Geom g, double *part) {
-  double acc = 0.0;
-  for (long long lin = (long long)blockIdx.x * RED_THREADS + threadIdx.x; lin < g.V;
-       lin += (long long)gridDim.x * RED_THREADS) {
-    const Site x = site_from_lin(g, lin);
+// Site order for lattice-wide reductions: warp w takes parity class w mod 2^Nd
+// and half-lattice sites [32 (w >> Nd), +32), so consecutive warps sweep all
+// classes of one window of half-lattice sites and the neighbour links a warp
+// needs were just brought into L2 by its sibling warps.  Coalescing is kept
+// (a warp reads 32 consecutive entries of one class).
+KLFT_D bool window_site(const Geom &g, long long t, Site &x, long long &lin) {
+  const int nsub = 1 << g.nd;
+  const long long w = t >> 5;
+  const int sub = (int)(w % nsub);
+  const long long hidx = (w / nsub) * 32 + (t & 31);
+  if (hidx >= g.Vh) return false;
+  long long r = hidx;
 #pragma unroll
+  for (int d = 0; d < 4; ++d) {
+    x.b[d] = (sub >> d) & 1;
+    x.h[d] = (int)(r % g.H[d]);
+    r /= g.H[d];
+  }
+  lin = (long long)sub * g.Vh + hidx;
+  return true;
+}
+
+KLFT_HD long long window_threads(const Geom &g) { return (long long)(1 << g.nd) * ((g.Vh + 31) / 32) * 32; }
+
+template <typename T> struct PlaqMinBlocks { static constexpr int v = 2; };
+template <> struct PlaqMinBlocks<double> { static constexpr int v = 1; };
+
+template <int NC, int ND, typename T>
+__global__ void __launch_bounds__(RED_THREADS, PlaqMinBlocks<T>::v) plaquette_kernel(Links<NC, T> U, Geom g, double *part) {
+  double acc = 0.0;
+  const long long nthr = window_threads(g);
+  for (long long t = (long long)blockIdx.x * RED_THREADS + threadIdx.x; t < nthr;
+       t += (long long)gridDim.x * RED_THREADS) {
+    Site x;
+    long long lin;
+    if (!window_site(g, t, x, lin)) continue;
+#pragma unroll 1
     for (int mu = 0; mu < ND; ++mu) {
       const Site xpmu = site_up(g, x, mu);
       const Mat<NC, T> umu = U.load(lin, mu);
-#pragma unroll
+#pragma unroll 1
       for (int nu = mu + 1; nu < ND; ++nu) {
         const Mat<NC, T> lmu = mul(umu, U.load(site_lin(g, xpmu), nu));
         const Mat<NC, T> lnu = mul(U.load(lin, nu), U.load(site_lin(g, site_up(g, x, nu)), mu));

@@ -138,10 +138,11 @@ __global__ void omega_kernel(Links<N, T> U, Geom g, ColGeom c, CField<N, T> om, 
   pol.store(col, O);
 }
 
-// U'_mu(col, row) for row < rows; one thread per entry, rows fastest.
+// U'_mu(col, row) for row < rows; one thread per entry, rows fastest.  The
+// products run in the link precision (Omega itself is an FP64 product).
 template <int N, typename T>
-__global__ void uprime_kernel(Links<N, T> U, Geom g, ColGeom c, CField<N, T> om, CField<N, T> pol,
-                              CField<N, T> up) {
+__global__ void __launch_bounds__(128) uprime_kernel(Links<N, T> U, Geom g, ColGeom c, CField<N, T> om,
+                                                     CField<N, T> pol, CField<N, T> up) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= c.ncols * c.rows) return;
   const long long col = t / c.rows;
@@ -149,13 +150,16 @@ __global__ void uprime_kernel(Links<N, T> U, Geom g, ColGeom c, CField<N, T> om,
   const int Ln = c.L[c.nu];
   const int b = row % Ln, k = row / Ln;
   const long long cp = col_shift(c, col, 1);
-  const Mat<N, double> u = to_d(U.load(site_lin(g, col_site(c, col, b)), c.mu));
-  Mat<N, double> v = mul_nd(mul(om.load(col * Ln + b), u), om.load(cp * Ln + b));
+  const Mat<N, T> u = U.load(site_lin(g, col_site(c, col, b)), c.mu);
+  Mat<N, T> v = mul_nd(mul(om.load_t(col * Ln + b), u), om.load_t(cp * Ln + b));
   if (k > 0) {
-    const Mat<N, double> P = pol.load(col), Pp = pol.load(cp);
+    const Mat<N, T> P = pol.load_t(col), Pp = pol.load_t(cp);
     for (int i = 0; i < k; ++i) v = mul_nd(mul(P, v), Pp);
   }
-  up.store(t, v);
+#pragma unroll
+  for (int a = 0; a < N; ++a)
+#pragma unroll
+    for (int bb = 0; bb < N; ++bb) up.p[(a * N + bb) * up.n + t] = v.e[a][bb];
 }
 
 constexpr int WL_THREADS = 128;
