@@ -95,6 +95,24 @@ klft_status klft_run_cycles(klft_lattice *lat, double beta, double delta, int nh
                             int ncycles, int measure_plaquette, const int *temporal_pairs, int npairs,
                             double *acc_out, double *plaq_out, double *w_out, double *device_ms);
 
+/* No counterpart in the reference.  klft_metropolis_sweeps without any
+ * allocation, for callers that cannot let the library allocate when they sweep:
+ * an application whose device memory is already handed to its own pool (a late
+ * cudaMalloc would fail) or a latency-critical loop that must not pay
+ * cudaMalloc/cudaFree (which can synchronise the whole device).  Same kernels,
+ * same random stream, same results as klft_metropolis_sweeps; the per-sweep
+ * acceptance counters live in a fixed device array of KLFT_NOALLOC_MAX_SWEEPS
+ * entries (8 KB, held on every GPU that loads the library until exit) instead
+ * of handle scratch.  nsweeps above that limit is rejected with KLFT_EINVAL.
+ * The lattice's device must be current.  The first call on a device looks up
+ * the array's device address (cudaGetSymbolAddress); make that first call
+ * before any stream capture.  All calls on a device share the array: each call
+ * clears the counters it uses, and because calls whose GPU work overlapped
+ * would race on them, a call holds a per-device lock until its stream is done. */
+#define KLFT_NOALLOC_MAX_SWEEPS 1024
+klft_status klft_metropolis_sweeps_noalloc(klft_lattice *lat, double beta, double delta, int nhits, int proposal,
+                                           double eps, int nsweeps, double *acc_out);
+
 /* Diagnostic with no reference counterpart: measured CUDA-core FMA throughput
  * (dtype 0: FP64, 1: FP32) of the current device in TFLOP/s, the roofline
  * denominator of this library's SU(N) kernels. */

@@ -40,6 +40,8 @@ SIGNATURES = {
     "klft_run_cycles": (C.c_int, [_vp, C.c_double, C.c_double, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, _ip,
                                   C.c_int, _dp, _dp, _dp, _dp]),
     "klft_peak_flops": (C.c_int, [C.c_int, _dp]),
+    "klft_metropolis_sweeps_noalloc": (C.c_int, [_vp, C.c_double, C.c_double, C.c_int, C.c_int, C.c_double, C.c_int,
+                                                 _dp]),
 }
 
 STATUS = {0: "KLFT_OK", 1: "KLFT_EINVAL", 2: "KLFT_ENOMEM", 3: "KLFT_ECUDA", 4: "KLFT_ETIMEOUT", 5: "KLFT_ENOTSUP"}
