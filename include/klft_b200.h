@@ -95,6 +95,37 @@ klft_status klft_run_cycles(klft_lattice *lat, double beta, double delta, int nh
                             int ncycles, int measure_plaquette, const int *temporal_pairs, int npairs,
                             double *acc_out, double *plaq_out, double *w_out, double *device_ms);
 
+/* ---------------------------------------------------------------- HMC
+ * Conventions of the reference (AdjointGroup.hpp), extended to SU(3) with the
+ * Gell-Mann generators t_a: U <- exp(i dt sum_a p_a t_a) U (U(1): e^{i dt p};
+ * SU(2): t_a = Pauli matrices), H = sum p^2/2 - (beta/Nc) sum_P Re Tr P,
+ * force F_a = (beta/Nc) Im Tr(t_a U S).  Momenta host layout:
+ * P[(site*Nd + mu)*ncomp + a], ncomp = 1, 3, 8 for U(1), SU(2), SU(3). */
+typedef enum {
+  KLFT_INTEGRATOR_REFERENCE_LEAPFROG = 0, /* Integrator.hpp:26-53: n_steps+1 gauge updates of tau/n_steps */
+  KLFT_INTEGRATOR_LEAPFROG = 1,           /* standard n-step leapfrog of length tau */
+  KLFT_INTEGRATOR_OMELYAN = 2             /* 2nd-order minimum norm (the LP_LEAPFROG slot, Integrator.hpp:10-13) */
+} klft_integrator;
+
+/* HMC::hmc_step (HMC.hpp:48-71), ntraj times: Gaussian momenta, integrate,
+ * dH in FP64, accept/reject on the device (reject restores the links).
+ * dH_out[k], accepted_out[k] per trajectory (either may be NULL). */
+klft_status klft_hmc_trajectories(klft_lattice *lat, double beta, double tau, int n_steps, int integrator,
+                                  int ntraj, double *dH_out, int *accepted_out);
+/* Leapfrog::integrate (Integrator.hpp:22-54) from the current momenta, then
+ * reunitarisation; no accept/reject. */
+klft_status klft_hmc_integrate(klft_lattice *lat, double beta, double tau, int n_steps, int integrator);
+/* HamiltonianField::randomize_momentum (HamiltonianField.hpp:50-59) from the
+ * (trajectory, site, mu) stream. */
+klft_status klft_hmc_refresh_momenta(klft_lattice *lat);
+klft_status klft_hmc_set_momenta(klft_lattice *lat, const double *host);
+klft_status klft_hmc_get_momenta(klft_lattice *lat, double *host);
+/* GaugeMonomial::derivative (GaugeMonomial.hpp:27-37): (beta/Nc) Adj(U S) per link, momenta layout. */
+klft_status klft_gauge_force(klft_lattice *lat, double beta, double *host_force);
+/* HamiltonianField::kinetic_energy (HamiltonianField.hpp:40-48) and the gauge
+ * monomial energy -(beta/Nc) sum_P Re Tr P (GaugeMonomial.hpp:19-25), FP64. */
+klft_status klft_hmc_energies(klft_lattice *lat, double beta, double *kinetic, double *gauge_action);
+
 /* No counterpart in the reference.  klft_metropolis_sweeps without any
  * allocation, for callers that cannot let the library allocate when they sweep:
  * an application whose device memory is already handed to its own pool (a late

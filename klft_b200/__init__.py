@@ -26,6 +26,7 @@ from ._lib import KlftError, check, lib
 PRECISION = {"fp64": 0, "mixed": 1}
 START = {"cold": 0, "hot": 1}
 PROPOSAL = {"reference": 0, "exp": 1}
+INTEGRATOR = {"reference": 0, "leapfrog": 1, "omelyan": 2}
 
 __all__ = [
     "GaugeField", "MetropolisParams", "GaugeObservableParams", "KlftError", "sweep_Metropolis",
@@ -152,6 +153,48 @@ class GaugeField:
                                     acc.ctypes.data_as(dp), plaq.ctypes.data_as(dp), w.ctypes.data_as(dp),
                                     C.byref(ms)))
         return acc[:ncycles], plaq[:ncycles], w[:ncycles, :len(p)], ms.value
+
+    # -- HMC
+    def ncomp(self) -> int:
+        return {1: 1, 2: 3, 3: 8}[self.nc]
+
+    def _pshape(self):
+        return (self.V, self.nd, self.ncomp())
+
+    def hmc(self, beta: float, tau: float, n_steps: int, ntraj: int = 1, integrator: str = "leapfrog"):
+        """ntraj HMC trajectories; returns (dH, accepted)."""
+        dH = np.zeros(max(ntraj, 1))
+        acc = np.zeros(max(ntraj, 1), dtype=np.int32)
+        check(lib().klft_hmc_trajectories(self._h, beta, tau, n_steps, INTEGRATOR[integrator], ntraj,
+                                          dH.ctypes.data_as(C.POINTER(C.c_double)),
+                                          acc.ctypes.data_as(C.POINTER(C.c_int))))
+        return dH[:ntraj], acc[:ntraj]
+
+    def hmc_integrate(self, beta: float, tau: float, n_steps: int, integrator: str = "leapfrog") -> None:
+        check(lib().klft_hmc_integrate(self._h, beta, tau, n_steps, INTEGRATOR[integrator]))
+
+    def refresh_momenta(self) -> None:
+        check(lib().klft_hmc_refresh_momenta(self._h))
+
+    def set_momenta(self, P: np.ndarray) -> None:
+        a = np.ascontiguousarray(P, dtype=np.float64)
+        assert a.size == int(np.prod(self._pshape()))
+        check(lib().klft_hmc_set_momenta(self._h, a.ctypes.data_as(C.POINTER(C.c_double))))
+
+    def momenta(self) -> np.ndarray:
+        a = np.zeros(self._pshape())
+        check(lib().klft_hmc_get_momenta(self._h, a.ctypes.data_as(C.POINTER(C.c_double))))
+        return a
+
+    def gauge_force(self, beta: float) -> np.ndarray:
+        a = np.zeros(self._pshape())
+        check(lib().klft_gauge_force(self._h, beta, a.ctypes.data_as(C.POINTER(C.c_double))))
+        return a
+
+    def hmc_energies(self, beta: float):
+        k, s = C.c_double(), C.c_double()
+        check(lib().klft_hmc_energies(self._h, beta, C.byref(k), C.byref(s)))
+        return k.value, s.value
 
     def unitarity(self) -> float:
         o = C.c_double()

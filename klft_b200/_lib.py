@@ -40,6 +40,13 @@ SIGNATURES = {
     "klft_run_cycles": (C.c_int, [_vp, C.c_double, C.c_double, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, _ip,
                                   C.c_int, _dp, _dp, _dp, _dp]),
     "klft_peak_flops": (C.c_int, [C.c_int, _dp]),
+    "klft_hmc_trajectories": (C.c_int, [_vp, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, _dp, _ip]),
+    "klft_hmc_integrate": (C.c_int, [_vp, C.c_double, C.c_double, C.c_int, C.c_int]),
+    "klft_hmc_refresh_momenta": (C.c_int, [_vp]),
+    "klft_hmc_set_momenta": (C.c_int, [_vp, _dp]),
+    "klft_hmc_get_momenta": (C.c_int, [_vp, _dp]),
+    "klft_gauge_force": (C.c_int, [_vp, C.c_double, _dp]),
+    "klft_hmc_energies": (C.c_int, [_vp, C.c_double, _dp, _dp]),
     "klft_metropolis_sweeps_noalloc": (C.c_int, [_vp, C.c_double, C.c_double, C.c_int, C.c_int, C.c_double, C.c_int,
                                                  _dp]),
 }

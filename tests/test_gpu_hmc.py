@@ -1,0 +1,85 @@
+"""GPU parity of HMC against the oracle (FP64 form to round-off; the mixed form
+to FP32 accuracy) and the HMC identities on the device."""
+import numpy as np
+import pytest
+
+from oracle.oracle import INTEGRATOR_LEAPFROG, INTEGRATOR_OMELYAN, INTEGRATOR_REFERENCE_LEAPFROG, Lat
+
+pytestmark = pytest.mark.gpu
+
+INTEG = {"reference": INTEGRATOR_REFERENCE_LEAPFROG, "leapfrog": INTEGRATOR_LEAPFROG, "omelyan": INTEGRATOR_OMELYAN}
+COMBOS = [(1, [6, 4, 4, 4]), (2, [4, 4, 4, 4]), (3, [4, 4, 2, 4]), (2, [6, 8]), (3, [4, 4, 4])]
+
+
+def gf(L, nc, precision="fp64", start="cold", seed=0):
+    import klft_b200
+    return klft_b200.GaugeField(L, nc, precision, start, seed)
+
+
+@pytest.mark.parametrize("nc,L", COMBOS)
+def test_force_and_momenta_match_oracle(oracle, nc, L):
+    lat = Lat(nc, L)
+    U = oracle.init(lat, True, 31)
+    g = gf(L, nc)
+    g.upload(U)
+    np.testing.assert_allclose(g.gauge_force(2.1), oracle.gauge_force(lat, U, 2.1), rtol=0, atol=1e-12)
+    g.set_stream(77, 3)
+    g.set_counters(0, 5)
+    g.refresh_momenta()
+    np.testing.assert_allclose(g.momenta(), oracle.momenta(lat, 77, 3, 5), rtol=0, atol=1e-14)
+    k, s = g.hmc_energies(2.1)
+    P = oracle.momenta(lat, 77, 3, 5)
+    assert k == pytest.approx(0.5 * np.sum(P * P), rel=1e-13)
+    assert s == pytest.approx(oracle.gauge_action(lat, U, 2.1), rel=1e-12)
+
+
+@pytest.mark.parametrize("nc,L", COMBOS)
+@pytest.mark.parametrize("integ", ["reference", "leapfrog", "omelyan"])
+def test_integrate_matches_oracle(oracle, nc, L, integ):
+    lat = Lat(nc, L)
+    U = oracle.init(lat, True, 41)
+    P = oracle.momenta(lat, 42, 0, 0)
+    g = gf(L, nc)
+    g.upload(U)
+    g.set_momenta(P)
+    g.hmc_integrate(2.0, 0.6, 6, integ)
+    oracle.integrate(lat, U, P, 2.0, 0.6, 6, INTEG[integ])
+    np.testing.assert_allclose(g.download(), U, rtol=0, atol=1e-11)
+    np.testing.assert_allclose(g.momenta(), P, rtol=0, atol=1e-10)
+
+
+@pytest.mark.parametrize("nc,L", COMBOS[:3])
+def test_trajectories_match_oracle(oracle, nc, L):
+    lat = Lat(nc, L)
+    U = oracle.init(lat, True, 51)
+    g = gf(L, nc)
+    g.upload(U)
+    g.set_stream(1001, 7)
+    beta = {1: 1.0, 2: 2.3, 3: 5.5}[nc]
+    dH_g, acc_g = g.hmc(beta, 1.0, 8, 4, "leapfrog")
+    dH_o, acc_o = oracle.hmc(lat, U, beta, 1.0, 8, INTEGRATOR_LEAPFROG, 1001, 7, 0, 4)
+    np.testing.assert_array_equal(acc_g, acc_o)
+    np.testing.assert_allclose(dH_g, dH_o, rtol=1e-8, atol=1e-9)
+    np.testing.assert_allclose(g.download(), U, rtol=0, atol=1e-10)
+    assert g.counters()[1] == 4
+
+
+def test_gpu_reversibility_and_mixed_dH():
+    import klft_b200
+    for precision, tol in (("fp64", 1e-11), ("mixed", 5e-5)):
+        g = klft_b200.GaugeField([8, 8, 8, 8], 2, precision, "hot", 3)
+        U0 = g.download()
+        g.refresh_momenta()
+        g.hmc_integrate(2.3, 0.5, 10, "leapfrog")
+        g.set_momenta(-g.momenta())
+        g.hmc_integrate(2.3, 0.5, 10, "leapfrog")
+        assert np.max(np.abs(g.download() - U0)) < tol
+        g.close()
+    # mixed form: dH of a trajectory within FP32 round-off of the FP64 form from the same state
+    out = {}
+    for precision in ("fp64", "mixed"):
+        g = klft_b200.GaugeField([8, 8, 8, 8], 2, precision, "hot", 5)
+        g.set_stream(12, 0)
+        out[precision] = g.hmc(2.3, 1.0, 20, 1, "leapfrog")[0][0]
+        g.close()
+    assert abs(out["fp64"] - out["mixed"]) < 2e-2
