@@ -126,6 +126,23 @@ klft_status klft_gauge_force(klft_lattice *lat, double beta, double *host_force)
  * monomial energy -(beta/Nc) sum_P Re Tr P (GaugeMonomial.hpp:19-25), FP64. */
 klft_status klft_hmc_energies(klft_lattice *lat, double beta, double *kinetic, double *gauge_action);
 
+/* ---------------------------------------------------------------- PTBC
+ * PTBCGaugeField set_defect / shift_defect (PTBCGaugeField.hpp:187-206): links
+ * mu = 0 at x0 = 0 whose spatial coordinates lie in pos + [0, len) (periodic)
+ * carry the factor c in the sweep (staples and dS).  len = 0 removes the defect.
+ * pos has Nd-1 entries (directions 1..Nd-1). */
+klft_status klft_lattice_set_defect(klft_lattice *lat, int len, const int *pos, double c);
+/* out2[n-1] = sum over plaquettes with n defect links of -(beta/Nc) Re Tr U_P
+ * (raw links), n = 1, 2: the only part of the action a swap changes. */
+klft_status klft_ptbc_defect_sums(klft_lattice *lat, double beta, double *out2);
+/* Replica swap (no counterpart in the reference, which defines the defect but
+ * never swaps): for k = 0..nrep-2 the replicas holding labels k and k+1 exchange
+ * labels with probability min(1, exp(-dS)), dS = sum_n (c_k^n - c_{k+1}^n)
+ * (A_n(b) - A_n(a)).  label_of_rep is updated in place, accepted[k] receives the
+ * decisions, and every replica's defect takes its new label's coefficient. */
+klft_status klft_ptbc_swap(klft_lattice *const *reps, int nrep, const double *c_of_label, int *label_of_rep,
+                           double beta, uint64_t seed, uint32_t cycle, int *accepted);
+
 /* No counterpart in the reference.  klft_metropolis_sweeps without any
  * allocation, for callers that cannot let the library allocate when they sweep:
  * an application whose device memory is already handed to its own pool (a late

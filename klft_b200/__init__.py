@@ -196,6 +196,16 @@ class GaugeField:
         check(lib().klft_hmc_energies(self._h, beta, C.byref(k), C.byref(s)))
         return k.value, s.value
 
+    # -- PTBC
+    def set_defect(self, length: int, pos=(0, 0, 0), c: float = 1.0) -> None:
+        p = (C.c_int * 3)(*(list(pos) + [0, 0, 0])[:3])
+        check(lib().klft_lattice_set_defect(self._h, length, p, c))
+
+    def defect_sums(self, beta: float) -> np.ndarray:
+        o = np.zeros(2)
+        check(lib().klft_ptbc_defect_sums(self._h, beta, o.ctypes.data_as(C.POINTER(C.c_double))))
+        return o
+
     def unitarity(self) -> float:
         o = C.c_double()
         check(lib().klft_unitarity(self._h, C.byref(o)))
@@ -203,6 +213,19 @@ class GaugeField:
 
     def reunitarize(self) -> None:
         check(lib().klft_reunitarize(self._h))
+
+
+def ptbc_swap(fields: Sequence[GaugeField], c_of_label, label_of_rep, beta: float, seed: int, cycle: int):
+    """Neighbour-label swap attempts over PTBC replicas; returns (labels, accepted)."""
+    n = len(fields)
+    reps = (C.c_void_p * n)(*[f.handle.value for f in fields])
+    c = np.ascontiguousarray(c_of_label, dtype=np.float64)
+    lab = np.ascontiguousarray(label_of_rep, dtype=np.int32).copy()
+    acc = np.zeros(max(n - 1, 1), dtype=np.int32)
+    check(lib().klft_ptbc_swap(reps, n, c.ctypes.data_as(C.POINTER(C.c_double)),
+                               lab.ctypes.data_as(C.POINTER(C.c_int)), beta, seed, cycle,
+                               acc.ctypes.data_as(C.POINTER(C.c_int))))
+    return lab, acc[: n - 1]
 
 
 # ------------------------------------------------------------------ reference-style API

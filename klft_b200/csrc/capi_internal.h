@@ -37,7 +37,7 @@ struct klft_lattice {
   uint32_t *d_counters = nullptr;  // [0] sweep, [1] trajectory, [2] cycle
   double *h_results = nullptr;     // pinned, KLFT_RESULT_SLOTS doubles
   klft::Scratch s_part, s_out, s_aux, s_stage, s_wl, s_hmc, s_gf, s_tab;
-  klft::Defect defect{0, 1, {0, 0, 0}, 1.0};
+  klft::Defect defect{0, 1, {0, 0, 0}, 1.0, nullptr};
   std::mutex mtx;
   int dtype() const { return precision == KLFT_PRECISION_FP64 ? 0 : 1; }
 };

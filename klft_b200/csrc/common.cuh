@@ -363,7 +363,15 @@ struct Defect {
   int len;
   int pos[3];
   double c;
+  const double *dyn_c;  // when set, the factor is read from device memory (replica swaps inside a graph)
 };
+KLFT_HD double defect_c(const Defect &df) {
+#ifdef __CUDA_ARCH__
+  return df.dyn_c ? *df.dyn_c : df.c;
+#else
+  return df.c;
+#endif
+}
 KLFT_HD bool in_defect(const Geom &g, const Defect &df, const Site &s, int mu) {
   if (!df.active || mu != 0) return false;
   if (2 * s.h[0] + s.b[0] != 0) return false;

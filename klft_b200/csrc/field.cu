@@ -133,7 +133,7 @@ __global__ void staple_field_kernel(Links<NC, T> U, Geom g, double *__restrict__
   const long long lex = t / ND;
   const int mu = (int)(t - lex * ND);
   const Site x = site_from_lex(g, lex);
-  Defect none{0, 1, {0, 0, 0}, 1.0};
+  Defect none{0, 1, {0, 0, 0}, 1.0, nullptr};
   const Mat<NC, T> S = staple<NC, ND, T>(U, g, x, mu, none);
   double *p = aos + t * (2 * NC * NC);
 #pragma unroll

@@ -51,7 +51,7 @@ __global__ void __launch_bounds__(128) force_update_kernel(Links<NC, T> U, T *P,
   const int mu = (int)(t / g.V);
   const long long lin = t - (long long)mu * g.V;
   const Site x = site_from_lin(g, lin);
-  const Defect none{0, 1, {0, 0, 0}, 1.0};
+  const Defect none{0, 1, {0, 0, 0}, 1.0, nullptr};
   const Mat<NC, T> M = mul(U.load(lin, mu), staple<NC, ND, T>(U, g, x, mu, none));
   constexpr int nc = Alg<NC>::n;
   T v[nc];

@@ -132,7 +132,7 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::v)
       for (int hit = 0; hit < a.nhits; ++hit) {
         const Mat<NC, T> rr = propose<T>(rng, (const Mat<NC, T> *)nullptr, a.delta, PROPOSAL_REFERENCE, 0.0);
         T dS = -bnc * (retr_mul(rr, M) - trO);
-        if (dlink) dS *= (T)df.c;
+        if (dlink) dS *= (T)defect_c(df);
         bool accept = dS < T(0);
         if (!accept) accept = rng.next() < (double)exp(-dS);
         if (accept) {
@@ -190,7 +190,7 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::v)
       for (int hit = 0; hit < a.nhits; ++hit) {
         rr = exp_proposal<T>(hs, h0 + hit, half_eps);
         T dS = -bnc * (retr_mul(rr, M) - trO);
-        if (dlink) dS *= (T)df.c;
+        if (dlink) dS *= (T)defect_c(df);
         bool accept = dS < T(0);
         if (!accept) accept = hs.accept_uniform(h0 + hit) < (double)exp(-dS);
         if (accept) {

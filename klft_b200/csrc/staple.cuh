@@ -11,7 +11,7 @@ namespace klft {
 template <int NC, typename T>
 KLFT_D Mat<NC, T> load_link(const Links<NC, T> &U, const Geom &g, const Site &s, int mu, const Defect &df) {
   Mat<NC, T> m = U.load(site_lin(g, s), mu);
-  if (df.active && in_defect(g, df, s, mu)) m = mscale(m, (T)df.c);
+  if (df.active && in_defect(g, df, s, mu)) m = mscale(m, (T)defect_c(df));
   return m;
 }
 

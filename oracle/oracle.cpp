@@ -899,6 +899,38 @@ int oracle_defect_action(int nc, int nd, const int *L, const double *U, const in
   return 0;
 }
 
+// Replica swap (project definition; the reference has a defect field but no swap).
+// Replica lattice r holds label label_of_rep[r] (coefficient c[label]).  For k =
+// 0..nrep-2 the lattices a, b holding labels k, k+1 swap labels with probability
+// min(1, exp(-dS)), dS = sum_{n=1,2} (c_k^n - c_{k+1}^n) (A_n(b) - A_n(a)), where
+// A[2r + n - 1] = sum over plaquettes of lattice r with n defect links of
+// s_P = -(beta/Nc) Re Tr U_P.  The uniform of pair k comes from the (cycle,
+// site = k) KIND_SWAP stream of chain 0.
+int oracle_ptbc_swap(int nrep, const double *c, const double *A, int *label_of_rep, uint64_t seed, uint32_t cycle,
+                     int *accepted) {
+  std::vector<int> rep_of_label(nrep);
+  for (int r = 0; r < nrep; ++r) rep_of_label[label_of_rep[r]] = r;
+  for (int k = 0; k + 1 < nrep; ++k) {
+    const int a = rep_of_label[k], b = rep_of_label[k + 1];
+    double dS = 0.0;
+    dS += (c[k] - c[k + 1]) * (A[2 * b] - A[2 * a]);
+    dS += (c[k] * c[k] - c[k + 1] * c[k + 1]) * (A[2 * b + 1] - A[2 * a + 1]);
+    bool acc = dS < 0.0;
+    if (!acc) {
+      Stream st(seed, 0, (uint32_t)k, cycle, KIND_SWAP, 0);
+      acc = st.next() < std::exp(-dS);
+    }
+    accepted[k] = acc ? 1 : 0;
+    if (acc) {
+      rep_of_label[k] = b;
+      rep_of_label[k + 1] = a;
+      label_of_rep[a] = k + 1;
+      label_of_rep[b] = k;
+    }
+  }
+  return 0;
+}
+
 int oracle_unitarity(int nc, int nd, const int *L, const double *U, double *out) {
   Geo g(nd, L);
   double worst = 0.0;

@@ -94,6 +94,16 @@ class Oracle:
         L.oracle_defect_sums.argtypes = [C.c_int, C.c_int, _ip, _dp, _ip, C.c_double, _dp]
         L.oracle_defect_action.argtypes = [C.c_int, C.c_int, _ip, _dp, _ip, C.c_double, C.c_double, _dp]
         L.oracle_unitarity.argtypes = [C.c_int, C.c_int, _ip, _dp, _dp]
+        L.oracle_ptbc_swap.argtypes = [C.c_int, _dp, _dp, _ip, C.c_uint64, C.c_uint32, _ip]
+
+    def ptbc_swap(self, c, A, label_of_rep, seed, cycle):
+        """Sequential neighbour-label swap attempts; returns (new labels, accepted per pair)."""
+        c = np.ascontiguousarray(c, dtype=np.float64)
+        A = np.ascontiguousarray(A, dtype=np.float64).reshape(-1)
+        lab = np.ascontiguousarray(label_of_rep, dtype=np.int32).copy()
+        acc = np.zeros(max(len(c) - 1, 1), dtype=np.int32)
+        self.lib.oracle_ptbc_swap(len(c), _d(c), _d(A), _i(lab), seed, cycle, _i(acc))
+        return lab, acc[: len(c) - 1]
 
     # -- random stream
     def philox(self, ctr, key):
