@@ -143,6 +143,18 @@ klft_status klft_ptbc_defect_sums(klft_lattice *lat, double beta, double *out2);
 klft_status klft_ptbc_swap(klft_lattice *const *reps, int nrep, const double *c_of_label, int *label_of_rep,
                            double beta, uint64_t seed, uint32_t cycle, int *accepted);
 
+/* ---------------------------------------------------------------- tuner
+ * tune_and_launch_for / readTuneCache / writeTuneCache (Tuner.hpp:73-358):
+ * with enabled != 0 (KLFT_TUNING=1) the first launch of a kernel under a key
+ * times the candidate launch shapes and keeps the fastest.  Cache file lines:
+ * "<rank> <key> <v0> ... <v{rank-1}>".  Results never depend on the shape. */
+klft_status klft_tuner_configure(int enabled, int verbosity);
+klft_status klft_tuner_read_cache(const char *path);
+klft_status klft_tuner_write_cache(const char *path);
+/* values[0..rank-1] of a cached key; *rank = 0 when absent. */
+klft_status klft_tuner_lookup(const char *key, int *values, int *rank);
+klft_status klft_tuner_clear(void);
+
 /* No counterpart in the reference.  klft_metropolis_sweeps without any
  * allocation, for callers that cannot let the library allocate when they sweep:
  * an application whose device memory is already handed to its own pool (a late

@@ -48,6 +48,11 @@ SIGNATURES = {
     "klft_gauge_force": (C.c_int, [_vp, C.c_double, _dp]),
     "klft_hmc_energies": (C.c_int, [_vp, C.c_double, _dp, _dp]),
     "klft_lattice_set_defect": (C.c_int, [_vp, C.c_int, _ip, C.c_double]),
+    "klft_tuner_configure": (C.c_int, [C.c_int, C.c_int]),
+    "klft_tuner_read_cache": (C.c_int, [C.c_char_p]),
+    "klft_tuner_write_cache": (C.c_int, [C.c_char_p]),
+    "klft_tuner_lookup": (C.c_int, [C.c_char_p, _ip, _ip]),
+    "klft_tuner_clear": (C.c_int, []),
     "klft_ptbc_defect_sums": (C.c_int, [_vp, C.c_double, _dp]),
     "klft_ptbc_swap": (C.c_int, [C.POINTER(_vp), C.c_int, _dp, _ip, C.c_double, C.c_uint64, C.c_uint32, _ip]),
     "klft_metropolis_sweeps_noalloc": (C.c_int, [_vp, C.c_double, C.c_double, C.c_int, C.c_int, C.c_double, C.c_int,

@@ -13,6 +13,7 @@
 #include "../../include/klft_b200.h"
 #include "capi_internal.h"
 #include "kernels.cuh"
+#include "tuner.h"
 
 using namespace klft;
 
@@ -165,7 +166,7 @@ klft_status klft_lattice_destroy(klft_lattice *lat) {
     LOCK(lat);
     if (lat->stream) cudaStreamSynchronize(lat->stream);
     for (Scratch *s : {&lat->s_part, &lat->s_out, &lat->s_aux, &lat->s_stage, &lat->s_wl, &lat->s_hmc,
-                        &lat->s_gf, &lat->s_tab})
+                        &lat->s_gf, &lat->s_tab, &lat->s_tune})
       s->release();
     if (lat->links) cudaFree(lat->links);
     if (lat->d_counters) cudaFree(lat->d_counters);
@@ -433,14 +434,40 @@ klft_status klft_run_cycles(klft_lattice *lat, double beta, double delta, int nh
 // ------------------------------------------------------------------ enqueue helpers
 namespace klft {
 
+// Block size of the sweep passes: 128 unless the tuner (KLFT_TUNING) picked
+// another; candidates are timed on a scratch copy of the links.
+static int sweep_block(klft_lattice *lat, const MetroArgs &a, const Defect &df, bool may_tune) {
+  if (!tuner_enabled()) return 128;
+  const std::string id = std::string("sweep_Metropolis_GaugeField_nc") + std::to_string(lat->nc) +
+                         (lat->dtype() == 0 ? "_fp64" : "_mixed") +
+                         (a.proposal == KLFT_PROPOSAL_EXP && lat->nc == 3 ? "_exp" : "_ref");
+  const std::string key = tune_key(id, lat->g.nd, lat->g.H);
+  auto time_fn = [&](int block) -> float {
+    const size_t off = (lat->link_bytes + 255) & ~(size_t)255;
+    if (lat->s_tune.ensure(off + 256) != cudaSuccess) return -1.f;
+    void *copy = lat->s_tune.ptr;
+    unsigned long long *dummy = (unsigned long long *)((char *)copy + off);
+    if (cudaMemcpyAsync(copy, lat->links, lat->link_bytes, cudaMemcpyDeviceToDevice, lat->stream) != cudaSuccess)
+      return -1.f;
+    return time_launches(lat->stream, 3, [&] {
+      return launch_metropolis_pass(lat->nc, lat->dtype(), copy, lat->g, 0, a, lat->d_counters, dummy, df, block,
+                                    lat->stream);
+    });
+  };
+  const int b = tuned_param(key, lat->g.nd, {32, 64, 128}, 128, time_fn, may_tune);
+  lat->s_tune.release();
+  return b;
+}
+
 klft_status enqueue_sweeps(klft_lattice *lat, double beta, double delta, int nhits, int proposal, double eps,
-                           int nsweeps, unsigned long long *d_nacc, const Defect &df) {
+                           int nsweeps, unsigned long long *d_nacc, const Defect &df, bool may_tune) {
   MetroArgs a{beta, delta, eps, nhits, proposal, lat->seed, lat->chain};
   const int nclass = 1 << lat->g.nd;
+  const int block = sweep_block(lat, a, df, may_tune);
   for (int k = 0; k < nsweeps; ++k) {
     for (int val = 0; val < nclass; ++val)
-      CK(launch_metropolis_pass(lat->nc, lat->dtype(), lat->links, lat->g, val, a, lat->d_counters, d_nacc + k, df, 0,
-                                lat->stream));
+      CK(launch_metropolis_pass(lat->nc, lat->dtype(), lat->links, lat->g, val, a, lat->d_counters, d_nacc + k, df,
+                                block, lat->stream));
     CK(launch_advance(lat->d_counters, lat->stream));
   }
   return KLFT_OK;

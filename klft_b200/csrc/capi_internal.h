@@ -36,7 +36,7 @@ struct klft_lattice {
   cudaStream_t stream = nullptr;
   uint32_t *d_counters = nullptr;  // [0] sweep, [1] trajectory, [2] cycle
   double *h_results = nullptr;     // pinned, KLFT_RESULT_SLOTS doubles
-  klft::Scratch s_part, s_out, s_aux, s_stage, s_wl, s_hmc, s_gf, s_tab;
+  klft::Scratch s_part, s_out, s_aux, s_stage, s_wl, s_hmc, s_gf, s_tab, s_tune;
   klft::Defect defect{0, 1, {0, 0, 0}, 1.0, nullptr};
   std::mutex mtx;
   int dtype() const { return precision == KLFT_PRECISION_FP64 ? 0 : 1; }
@@ -44,8 +44,9 @@ struct klft_lattice {
 
 namespace klft {
 klft_status lattice_sync(klft_lattice *lat);
+// may_tune = false: use only tuned values already known (no timing, no scratch)
 klft_status enqueue_sweeps(klft_lattice *lat, double beta, double delta, int nhits, int proposal, double eps,
-                           int nsweeps, unsigned long long *d_nacc, const Defect &df);
+                           int nsweeps, unsigned long long *d_nacc, const Defect &df, bool may_tune = true);
 klft_status enqueue_plaquette(klft_lattice *lat, int slot);
 double normalize_plaquette(const klft_lattice *lat, double sum);
 double normalize_wilson(const klft_lattice *lat, double sum);

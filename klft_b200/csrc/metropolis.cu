@@ -223,9 +223,9 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::v)
 
 template <int NC, int ND, typename T>
 static cudaError_t launch_t(void *links, const Geom &g, int val, const MetroArgs &a, const uint32_t *d_sweep,
-                            unsigned long long *d_nacc, const Defect &df, cudaStream_t st) {
+                            unsigned long long *d_nacc, const Defect &df, int block, cudaStream_t st) {
   Links<NC, T> U{(cx<T> *)links, g.V};
-  const int block = 128;
+  if (block != 32 && block != 64 && block != 128) block = 128;  // the kernels are built for <= 128 threads
   const unsigned grid = (unsigned)((g.Vh + block - 1) / block);
   if constexpr (NC == 3) {
     if (a.proposal == PROPOSAL_EXP) {
@@ -239,29 +239,30 @@ static cudaError_t launch_t(void *links, const Geom &g, int val, const MetroArgs
 
 template <int NC, typename T>
 static cudaError_t launch_nd(int nd, void *links, const Geom &g, int val, const MetroArgs &a,
-                             const uint32_t *d_sweep, unsigned long long *d_nacc, const Defect &df, cudaStream_t st) {
+                             const uint32_t *d_sweep, unsigned long long *d_nacc, const Defect &df, int block,
+                             cudaStream_t st) {
   switch (nd) {
-    case 2: return launch_t<NC, 2, T>(links, g, val, a, d_sweep, d_nacc, df, st);
-    case 3: return launch_t<NC, 3, T>(links, g, val, a, d_sweep, d_nacc, df, st);
-    case 4: return launch_t<NC, 4, T>(links, g, val, a, d_sweep, d_nacc, df, st);
+    case 2: return launch_t<NC, 2, T>(links, g, val, a, d_sweep, d_nacc, df, block, st);
+    case 3: return launch_t<NC, 3, T>(links, g, val, a, d_sweep, d_nacc, df, block, st);
+    case 4: return launch_t<NC, 4, T>(links, g, val, a, d_sweep, d_nacc, df, block, st);
   }
   return cudaErrorInvalidValue;
 }
 
 cudaError_t launch_metropolis_pass(int nc, int dtype, void *links, const Geom &g, int val, const MetroArgs &a,
-                                   const uint32_t *d_sweep, unsigned long long *d_nacc, const Defect &df, int,
+                                   const uint32_t *d_sweep, unsigned long long *d_nacc, const Defect &df, int block,
                                    cudaStream_t st) {
   if (dtype == 0) {
     switch (nc) {
-      case 1: return launch_nd<1, double>(g.nd, links, g, val, a, d_sweep, d_nacc, df, st);
-      case 2: return launch_nd<2, double>(g.nd, links, g, val, a, d_sweep, d_nacc, df, st);
-      case 3: return launch_nd<3, double>(g.nd, links, g, val, a, d_sweep, d_nacc, df, st);
+      case 1: return launch_nd<1, double>(g.nd, links, g, val, a, d_sweep, d_nacc, df, block, st);
+      case 2: return launch_nd<2, double>(g.nd, links, g, val, a, d_sweep, d_nacc, df, block, st);
+      case 3: return launch_nd<3, double>(g.nd, links, g, val, a, d_sweep, d_nacc, df, block, st);
     }
   } else {
     switch (nc) {
-      case 1: return launch_nd<1, float>(g.nd, links, g, val, a, d_sweep, d_nacc, df, st);
-      case 2: return launch_nd<2, float>(g.nd, links, g, val, a, d_sweep, d_nacc, df, st);
-      case 3: return launch_nd<3, float>(g.nd, links, g, val, a, d_sweep, d_nacc, df, st);
+      case 1: return launch_nd<1, float>(g.nd, links, g, val, a, d_sweep, d_nacc, df, block, st);
+      case 2: return launch_nd<2, float>(g.nd, links, g, val, a, d_sweep, d_nacc, df, block, st);
+      case 3: return launch_nd<3, float>(g.nd, links, g, val, a, d_sweep, d_nacc, df, block, st);
     }
   }
   return cudaErrorInvalidValue;

@@ -84,7 +84,9 @@ extern "C" klft_status klft_metropolis_sweeps_noalloc(klft_lattice *lat, double 
   const size_t bytes = (size_t)nsweeps * sizeof(unsigned long long);
   e = cudaMemsetAsync(d_acc, 0, bytes, lat->stream);
   if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(static counters)");
-  s = enqueue_sweeps(lat, beta, delta, nhits, proposal, eps, nsweeps, d_acc, lat->defect);
+  // may_tune = false: a launch shape the tuner already chose is used, but no
+  // tuning (which would allocate a scratch copy of the links) starts here
+  s = enqueue_sweeps(lat, beta, delta, nhits, proposal, eps, nsweeps, d_acc, lat->defect, false);
   if (s != KLFT_OK) {
     cudaStreamSynchronize(lat->stream);
     return s;
