@@ -143,6 +143,34 @@ klft_status klft_ptbc_defect_sums(klft_lattice *lat, double beta, double *out2);
 klft_status klft_ptbc_swap(klft_lattice *const *reps, int nrep, const double *c_of_label, int *label_of_rep,
                            double beta, uint64_t seed, uint32_t cycle, int *accepted);
 
+/* ---------------------------------------------------------------- batches
+ * No counterpart in the reference (which runs one lattice per process): many
+ * chains of any group, dimension, extents and precision, plus optional PTBC
+ * replicas, advanced together.  One cycle = one Metropolis sweep of every chain
+ * (reference sweep order per chain), then replica swap attempts, then (when
+ * asked) the plaquette of every chain.  With use_graph the cycle is captured
+ * once as a CUDA graph and replayed.  Results are identical to running each
+ * chain alone with klft_metropolis_sweeps / klft_ptbc_swap.  Member lattices
+ * must not be used by other calls while klft_batch_run runs. */
+typedef struct klft_batch klft_batch;
+klft_status klft_batch_create(klft_batch **out);
+klft_status klft_batch_destroy(klft_batch *b);
+/* Adds an existing lattice (owned by the caller) with its Metropolis parameters. */
+klft_status klft_batch_add_chain(klft_batch *b, klft_lattice *lat, double beta, double delta, int nhits,
+                                 int proposal, double eps, int *chain_id);
+/* Marks nrep chains (each with a defect set) as PTBC replicas; replica r starts
+ * with label r and coefficient c_of_label[r]; swaps use the (cycle, pair)
+ * stream of swap_seed. */
+klft_status klft_batch_set_ptbc(klft_batch *b, const int *chain_ids, int nrep, const double *c_of_label,
+                                double beta, uint64_t swap_seed);
+/* ncycles cycles: acc_out[c*nchains + i], plaq_out[c*nchains + i] (normalised as
+ * GaugePlaquette), labels_out[c*nrep + r] (label of replica r after cycle c);
+ * device_ms = CUDA-event time of the cycles.  Outputs may be NULL. */
+klft_status klft_batch_run(klft_batch *b, int ncycles, int measure_plaquette, int use_graph, double *acc_out,
+                           double *plaq_out, int *labels_out, double *device_ms);
+/* accepted swaps per neighbouring label pair since klft_batch_set_ptbc (nrep-1 entries). */
+klft_status klft_batch_swap_stats(klft_batch *b, unsigned long long *accepted_per_pair);
+
 /* ---------------------------------------------------------------- tuner
  * tune_and_launch_for / readTuneCache / writeTuneCache (Tuner.hpp:73-358):
  * with enabled != 0 (KLFT_TUNING=1) the first launch of a kernel under a key

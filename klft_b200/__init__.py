@@ -228,6 +228,60 @@ def ptbc_swap(fields: Sequence[GaugeField], c_of_label, label_of_rep, beta: floa
     return lab, acc[: n - 1]
 
 
+class Batch:
+    """Chains (and PTBC replicas) advanced together; one cycle per graph replay."""
+
+    def __init__(self):
+        h = C.c_void_p()
+        check(lib().klft_batch_create(C.byref(h)))
+        self._h = h
+        self.fields: List[GaugeField] = []
+        self.nrep = 0
+
+    def add(self, field: GaugeField, beta: float, delta: float, nhits: int, proposal: str = "reference",
+            eps: float = 0.0) -> int:
+        cid = C.c_int()
+        check(lib().klft_batch_add_chain(self._h, field.handle, beta, delta, nhits, PROPOSAL[proposal], eps,
+                                         C.byref(cid)))
+        self.fields.append(field)
+        return cid.value
+
+    def set_ptbc(self, chain_ids, c_of_label, beta: float, swap_seed: int) -> None:
+        ids = np.ascontiguousarray(chain_ids, dtype=np.int32)
+        c = np.ascontiguousarray(c_of_label, dtype=np.float64)
+        check(lib().klft_batch_set_ptbc(self._h, ids.ctypes.data_as(C.POINTER(C.c_int)), len(ids),
+                                        c.ctypes.data_as(C.POINTER(C.c_double)), beta, swap_seed))
+        self.nrep = len(ids)
+
+    def run(self, ncycles: int, measure_plaquette: bool = True, use_graph: bool = True):
+        """Returns (acc[ncycles, nchains], plaq[ncycles, nchains], labels[ncycles, nrep], device_ms)."""
+        n = len(self.fields)
+        acc = np.zeros((ncycles, n))
+        plaq = np.zeros((ncycles, n))
+        lab = np.zeros((ncycles, max(self.nrep, 1)), dtype=np.int32)
+        ms = C.c_double()
+        dp = C.POINTER(C.c_double)
+        check(lib().klft_batch_run(self._h, ncycles, int(measure_plaquette), int(use_graph), acc.ctypes.data_as(dp),
+                                   plaq.ctypes.data_as(dp), lab.ctypes.data_as(C.POINTER(C.c_int)), C.byref(ms)))
+        return acc, plaq, lab[:, : self.nrep], ms.value
+
+    def swap_stats(self) -> np.ndarray:
+        a = np.zeros(max(self.nrep - 1, 1), dtype=np.uint64)
+        check(lib().klft_batch_swap_stats(self._h, a.ctypes.data_as(C.POINTER(C.c_ulonglong))))
+        return a[: max(self.nrep - 1, 0)]
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib().klft_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 # ------------------------------------------------------------------ reference-style API
 @dataclass
 class MetropolisParams:

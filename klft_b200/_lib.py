@@ -48,6 +48,12 @@ SIGNATURES = {
     "klft_gauge_force": (C.c_int, [_vp, C.c_double, _dp]),
     "klft_hmc_energies": (C.c_int, [_vp, C.c_double, _dp, _dp]),
     "klft_lattice_set_defect": (C.c_int, [_vp, C.c_int, _ip, C.c_double]),
+    "klft_batch_create": (C.c_int, [C.POINTER(_vp)]),
+    "klft_batch_destroy": (C.c_int, [_vp]),
+    "klft_batch_add_chain": (C.c_int, [_vp, _vp, C.c_double, C.c_double, C.c_int, C.c_int, C.c_double, _ip]),
+    "klft_batch_set_ptbc": (C.c_int, [_vp, _ip, C.c_int, _dp, C.c_double, C.c_uint64]),
+    "klft_batch_run": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, _dp, _dp, _ip, _dp]),
+    "klft_batch_swap_stats": (C.c_int, [_vp, C.POINTER(C.c_ulonglong)]),
     "klft_tuner_configure": (C.c_int, [C.c_int, C.c_int]),
     "klft_tuner_read_cache": (C.c_int, [C.c_char_p]),
     "klft_tuner_write_cache": (C.c_int, [C.c_char_p]),

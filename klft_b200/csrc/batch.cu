@@ -1,0 +1,497 @@
+// batch.cu -- many independent chains and PTBC replicas, of uneven groups and
+// extents, advanced together; one cycle (a sweep of every chain, replica swap
+// attempts, plaquette of every chain) is captured once as a CUDA graph and
+// replayed.
+//
+// Chains are grouped by kernel variant (Nc, Nd, precision, proposal, defect).
+// A group's chain table travels by value in the kernel parameters (up to
+// BATCH_MAX chains, read from the constant bank); its CTAs are laid out chain
+// after chain, and a CTA finds its chain by a binary search on the table's
+// block offsets.  Parity classes are the unit of ordering: for each class val
+// one launch per group updates that class of every chain in the group, so the
+// reference's sweep order holds for every chain.  Per-cycle results (accepted
+// hits, plaquette sums, replica labels) land in device slots selected by a
+// device counter, so the captured graph is replayed unchanged.  Replica swaps
+// run on the device (ptbc.cu) and write each replica's defect coefficient,
+// which the sweep kernels read through Defect::dyn_c.
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "../../include/klft_b200.h"
+#include "capi_internal.h"
+#include "kernels.cuh"
+#include "metropolis_site.cuh"
+
+namespace klft {
+
+constexpr int BATCH_MAX = 64;
+
+struct ChainDesc {
+  void *links;
+  uint32_t *ctr;  // the chain's counters ([0] = sweep)
+  Geom g;
+  MetroArgs a;
+  Defect df;
+  int index;        // chain id in the batch
+  int block_begin;  // first CTA of this chain in the launch
+};
+
+struct ChainTable {
+  int n;
+  int nchains_total;
+  ChainDesc c[BATCH_MAX];
+};
+
+KLFT_D int find_chain(const ChainTable &tab) {
+  int lo = 0, hi = tab.n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (tab.c[mid].block_begin <= (int)blockIdx.x) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+template <int NC, int ND, typename T, bool EXP, bool DF>
+__global__ void __launch_bounds__(128, MinBlocks<T>::v)
+    multi_pass_kernel(const __grid_constant__ ChainTable tab, int val, unsigned long long *nacc_slots,
+                      const uint32_t *__restrict__ slot) {
+  const int ci = find_chain(tab);
+  const ChainDesc &c = tab.c[ci];
+  const long long t = (long long)(blockIdx.x - c.block_begin) * blockDim.x + threadIdx.x;
+  int nacc = 0;
+  if (t < c.g.Vh) {
+    const Links<NC, T> U{(cx<T> *)c.links, c.g.V};
+    const Site x = pass_site(c.g, t, val, ND);
+    if constexpr (EXP && NC == 3) nacc = site_update_exp<ND, T, DF>(U, c.g, x, c.a, *c.ctr, c.df);
+    else nacc = site_update_ref<NC, ND, T, DF>(U, c.g, x, c.a, *c.ctr, c.df);
+  }
+  add_accepts(nacc, nacc_slots + (size_t)(*slot) * tab.nchains_total + c.index);
+}
+
+__global__ void batch_advance_kernel(uint32_t *const *ctrs, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) ctrs[i][0] += 1u;
+}
+
+__global__ void batch_slot_kernel(uint32_t *slot, uint32_t *cycle) {
+  *slot += 1u;
+  *cycle += 1u;
+}
+
+__global__ void copy_labels_kernel(const int *labels, int n, int *dst, const uint32_t *slot) {
+  const int i = threadIdx.x;
+  if (i < n) dst[(size_t)(*slot) * n + i] = labels[i];
+}
+
+__global__ void copy_slot_kernel(const double *src, double *dst, const uint32_t *slot, int stride, int index) {
+  dst[(size_t)(*slot) * stride + index] = *src;
+}
+
+// declared in ptbc.cu
+cudaError_t launch_defect_sums(int nc, int dtype, const void *links, const Geom &g, const Defect &df, double beta,
+                               double *d_part, double *d_out, cudaStream_t st);
+int defect_sums_blocks(const Geom &g);
+__global__ void ptbc_swap_kernel(int nrep, const double *c_of_label, const double *A, int *label_of_rep,
+                                 int *rep_of_label, double *c_of_rep, uint64_t seed, const uint32_t *cycle_ctr,
+                                 unsigned long long *swap_acc);
+
+}  // namespace klft
+
+using namespace klft;
+
+#define CK(call)                                        \
+  do {                                                  \
+    cudaError_t e_ = (call);                            \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
+  } while (0)
+
+struct klft_batch {
+  struct Chain {
+    klft_lattice *lat;
+    double beta, delta, eps;
+    int nhits, proposal;
+  };
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::vector<Chain> chains;
+  // PTBC
+  std::vector<int> reps;  // chain ids of the replicas, replica r = reps[r]
+  std::vector<double> c_of_label;
+  double ptbc_beta = 0.0;
+  uint64_t swap_seed = 0;
+  // device state
+  uint32_t *d_slot = nullptr;   // [0] result slot, [1] cycle counter (swap stream step)
+  uint32_t **d_ctrs = nullptr;  // per-chain counter pointers
+  double *d_c_of_label = nullptr, *d_c_of_rep = nullptr, *d_A = nullptr, *d_part = nullptr;
+  int *d_label_of_rep = nullptr, *d_rep_of_label = nullptr;
+  unsigned long long *d_swap_acc = nullptr;
+  klft::Scratch s_nacc, s_plaq, s_labels, s_ppart;
+  int cap = 0;  // result slots
+  bool dirty = true;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int graph_measure = -1;
+  std::mutex mtx;
+
+  void drop_graph() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    exec = nullptr;
+    graph = nullptr;
+  }
+};
+
+namespace {
+
+struct GroupKey {
+  int nc, nd, dtype, exp, df;
+  bool operator==(const GroupKey &o) const {
+    return nc == o.nc && nd == o.nd && dtype == o.dtype && exp == o.exp && df == o.df;
+  }
+};
+
+template <int NC, int ND, typename T, bool EXP, bool DF>
+cudaError_t launch_group_t(const ChainTable &tab, int blocks, int val, unsigned long long *nacc, const uint32_t *slot,
+                           cudaStream_t st) {
+  multi_pass_kernel<NC, ND, T, EXP, DF><<<blocks, 128, 0, st>>>(tab, val, nacc, slot);
+  return cudaGetLastError();
+}
+
+template <int NC, int ND, typename T>
+cudaError_t launch_group_nd(const GroupKey &k, const ChainTable &tab, int blocks, int val, unsigned long long *nacc,
+                            const uint32_t *slot, cudaStream_t st) {
+  if (k.exp) {
+    if (k.df) return launch_group_t<NC, ND, T, true, true>(tab, blocks, val, nacc, slot, st);
+    return launch_group_t<NC, ND, T, true, false>(tab, blocks, val, nacc, slot, st);
+  }
+  if (k.df) return launch_group_t<NC, ND, T, false, true>(tab, blocks, val, nacc, slot, st);
+  return launch_group_t<NC, ND, T, false, false>(tab, blocks, val, nacc, slot, st);
+}
+
+template <int NC, typename T>
+cudaError_t launch_group_nc(const GroupKey &k, const ChainTable &tab, int blocks, int val, unsigned long long *nacc,
+                            const uint32_t *slot, cudaStream_t st) {
+  if (k.nd == 2) return launch_group_nd<NC, 2, T>(k, tab, blocks, val, nacc, slot, st);
+  if (k.nd == 3) return launch_group_nd<NC, 3, T>(k, tab, blocks, val, nacc, slot, st);
+  return launch_group_nd<NC, 4, T>(k, tab, blocks, val, nacc, slot, st);
+}
+
+cudaError_t launch_group(const GroupKey &k, const ChainTable &tab, int blocks, int val, unsigned long long *nacc,
+                         const uint32_t *slot, cudaStream_t st) {
+  if (k.dtype == 0) {
+    if (k.nc == 1) return launch_group_nc<1, double>(k, tab, blocks, val, nacc, slot, st);
+    if (k.nc == 2) return launch_group_nc<2, double>(k, tab, blocks, val, nacc, slot, st);
+    return launch_group_nc<3, double>(k, tab, blocks, val, nacc, slot, st);
+  }
+  if (k.nc == 1) return launch_group_nc<1, float>(k, tab, blocks, val, nacc, slot, st);
+  if (k.nc == 2) return launch_group_nc<2, float>(k, tab, blocks, val, nacc, slot, st);
+  return launch_group_nc<3, float>(k, tab, blocks, val, nacc, slot, st);
+}
+
+struct Group {
+  GroupKey key;
+  std::vector<std::unique_ptr<ChainTable>> tables;
+  std::vector<int> blocks;
+};
+
+// Enqueue one cycle on b->stream (recorded into the graph by the caller).
+klft_status enqueue_cycle(klft_batch *b, int measure) {
+  const int n = (int)b->chains.size();
+  std::vector<Group> groups;
+  int replica_of_chain_none = -1;
+  (void)replica_of_chain_none;
+  for (int i = 0; i < n; ++i) {
+    const auto &ch = b->chains[i];
+    klft_lattice *lat = ch.lat;
+    int rep = -1;
+    for (size_t r = 0; r < b->reps.size(); ++r)
+      if (b->reps[r] == i) rep = (int)r;
+    GroupKey key{lat->nc, lat->g.nd, lat->dtype(), (lat->nc == 3 && ch.proposal == KLFT_PROPOSAL_EXP) ? 1 : 0,
+                 lat->defect.active ? 1 : 0};
+    Group *grp = nullptr;
+    for (auto &gg : groups)
+      if (gg.key == key) grp = &gg;
+    if (!grp) {
+      groups.push_back(Group{key, {}, {}});
+      grp = &groups.back();
+    }
+    if (grp->tables.empty() || grp->tables.back()->n == BATCH_MAX) {
+      grp->tables.emplace_back(new ChainTable());
+      std::memset(grp->tables.back().get(), 0, sizeof(ChainTable));
+      grp->tables.back()->nchains_total = n;
+      grp->blocks.push_back(0);
+    }
+    ChainTable &tab = *grp->tables.back();
+    ChainDesc &d = tab.c[tab.n++];
+    d.links = lat->links;
+    d.ctr = lat->d_counters;
+    d.g = lat->g;
+    d.a = MetroArgs{ch.beta, ch.delta, ch.eps, ch.nhits, ch.proposal, lat->seed, lat->chain};
+    d.df = lat->defect;
+    if (rep >= 0) d.df.dyn_c = b->d_c_of_rep + rep;
+    d.index = i;
+    d.block_begin = grp->blocks.back();
+    grp->blocks.back() += (int)((lat->g.Vh + 127) / 128);
+  }
+  unsigned long long *nacc = (unsigned long long *)b->s_nacc.ptr;
+  int maxnd = 0;
+  for (auto &gg : groups) maxnd = gg.key.nd > maxnd ? gg.key.nd : maxnd;
+  for (int val = 0; val < (1 << maxnd); ++val)
+    for (auto &gg : groups) {
+      if (val >= (1 << gg.key.nd)) continue;
+      for (size_t t = 0; t < gg.tables.size(); ++t)
+        CK(launch_group(gg.key, *gg.tables[t], gg.blocks[t], val, nacc, b->d_slot, b->stream));
+    }
+  batch_advance_kernel<<<(n + 127) / 128, 128, 0, b->stream>>>(b->d_ctrs, n);
+  CK(cudaGetLastError());
+  if (!b->reps.empty()) {
+    const int nrep = (int)b->reps.size();
+    for (int r = 0; r < nrep; ++r) {
+      klft_lattice *lat = b->chains[b->reps[r]].lat;
+      CK(launch_defect_sums(lat->nc, lat->dtype(), lat->links, lat->g, lat->defect, b->ptbc_beta, b->d_part,
+                            b->d_A + 2 * r, b->stream));
+    }
+    ptbc_swap_kernel<<<1, 1, 0, b->stream>>>(nrep, b->d_c_of_label, b->d_A, b->d_label_of_rep, b->d_rep_of_label,
+                                             b->d_c_of_rep, b->swap_seed, b->d_slot + 1, b->d_swap_acc);
+    CK(cudaGetLastError());
+    copy_labels_kernel<<<1, 64, 0, b->stream>>>(b->d_label_of_rep, nrep, (int *)b->s_labels.ptr, b->d_slot);
+    CK(cudaGetLastError());
+  }
+  if (measure) {
+    double *plaq = (double *)b->s_plaq.ptr;
+    for (int i = 0; i < n; ++i) {
+      klft_lattice *lat = b->chains[i].lat;
+      const int nblk = plaquette_blocks(lat->g);
+      double *part = (double *)b->s_ppart.ptr;
+      CK(launch_plaquette(lat->nc, lat->dtype(), lat->links, lat->g, part, nblk, part + nblk, b->stream));
+      copy_slot_kernel<<<1, 1, 0, b->stream>>>(part + nblk, plaq, b->d_slot, n, i);
+      CK(cudaGetLastError());
+    }
+  }
+  batch_slot_kernel<<<1, 1, 0, b->stream>>>(b->d_slot, b->d_slot + 1);
+  CK(cudaGetLastError());
+  return KLFT_OK;
+}
+
+klft_status prepare(klft_batch *b, int ncycles) {
+  const int n = (int)b->chains.size();
+  if (ncycles > b->cap) {
+    b->cap = ncycles;
+    b->dirty = true;
+  }
+  CK(b->s_nacc.ensure((size_t)b->cap * n * sizeof(unsigned long long)));
+  CK(b->s_plaq.ensure((size_t)b->cap * n * sizeof(double)));
+  CK(b->s_labels.ensure((size_t)b->cap * (b->reps.empty() ? 1 : b->reps.size()) * sizeof(int)));
+  int maxblk = 1;
+  for (auto &ch : b->chains) {
+    const int nb = plaquette_blocks(ch.lat->g);
+    maxblk = nb > maxblk ? nb : maxblk;
+  }
+  CK(b->s_ppart.ensure((size_t)(maxblk + 1) * sizeof(double)));
+  if (!b->d_ctrs) {
+    CK(cudaMalloc(&b->d_ctrs, BATCH_MAX * 64 * sizeof(uint32_t *)));
+  }
+  std::vector<uint32_t *> ctrs;
+  for (auto &ch : b->chains) ctrs.push_back(ch.lat->d_counters);
+  CK(cudaMemcpyAsync(b->d_ctrs, ctrs.data(), ctrs.size() * sizeof(uint32_t *), cudaMemcpyHostToDevice, b->stream));
+  return KLFT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+klft_status klft_batch_create(klft_batch **out) {
+  if (!out) return fail(KLFT_EINVAL, "klft_batch_create: null pointer");
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return fail(KLFT_ECUDA, "klft_batch_create: no CUDA device available");
+  klft_batch *b = new klft_batch();
+  cudaGetDevice(&b->device);
+  cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_slot, 4 * sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaMemsetAsync(b->d_slot, 0, 4 * sizeof(uint32_t), b->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+  if (e != cudaSuccess) {
+    klft_status s = cuda_fail(e, "klft_batch_create");
+    klft_batch_destroy(b);
+    return s;
+  }
+  *out = b;
+  return KLFT_OK;
+}
+
+klft_status klft_batch_destroy(klft_batch *b) {
+  if (!b) return KLFT_OK;
+  {
+    std::lock_guard<std::mutex> g(b->mtx);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    b->drop_graph();
+    for (klft::Scratch *s : {&b->s_nacc, &b->s_plaq, &b->s_labels, &b->s_ppart}) s->release();
+    for (void *p : {(void *)b->d_slot, (void *)b->d_ctrs, (void *)b->d_c_of_label, (void *)b->d_c_of_rep,
+                    (void *)b->d_A, (void *)b->d_part, (void *)b->d_label_of_rep, (void *)b->d_rep_of_label,
+                    (void *)b->d_swap_acc})
+      if (p) cudaFree(p);
+    if (b->stream) cudaStreamDestroy(b->stream);
+  }
+  delete b;
+  return KLFT_OK;
+}
+
+klft_status klft_batch_add_chain(klft_batch *b, klft_lattice *lat, double beta, double delta, int nhits, int proposal,
+                                 double eps, int *chain_id) {
+  if (!b || !lat) return fail(KLFT_EINVAL, "klft_batch_add_chain: null handle");
+  if (nhits < 0) return fail(KLFT_EINVAL, "klft_batch_add_chain: negative nHits");
+  if (proposal != KLFT_PROPOSAL_REFERENCE && proposal != KLFT_PROPOSAL_EXP)
+    return fail(KLFT_EINVAL, "klft_batch_add_chain: unknown proposal %d", proposal);
+  if (lat->nc == 3 && proposal == KLFT_PROPOSAL_REFERENCE && !(delta > 0.0))
+    return fail(KLFT_EINVAL, "klft_batch_add_chain: the reference SU(3) proposal needs delta > 0");
+  if (lat->device != b->device) return fail(KLFT_EINVAL, "klft_batch_add_chain: lattice on another device");
+  std::lock_guard<std::mutex> g(b->mtx);
+  if (b->chains.size() >= (size_t)BATCH_MAX * 64) return fail(KLFT_EINVAL, "klft_batch_add_chain: too many chains");
+  for (auto &ch : b->chains)
+    if (ch.lat == lat) return fail(KLFT_EINVAL, "klft_batch_add_chain: lattice already in the batch");
+  b->chains.push_back({lat, beta, delta, eps, nhits, proposal});
+  if (chain_id) *chain_id = (int)b->chains.size() - 1;
+  b->dirty = true;
+  return KLFT_OK;
+}
+
+klft_status klft_batch_set_ptbc(klft_batch *b, const int *chain_ids, int nrep, const double *c_of_label, double beta,
+                                uint64_t swap_seed) {
+  if (!b || !chain_ids || !c_of_label || nrep < 1 || nrep > 64)
+    return fail(KLFT_EINVAL, "klft_batch_set_ptbc: bad arguments (1 <= nrep <= 64)");
+  std::lock_guard<std::mutex> g(b->mtx);
+  for (int r = 0; r < nrep; ++r) {
+    if (chain_ids[r] < 0 || chain_ids[r] >= (int)b->chains.size())
+      return fail(KLFT_EINVAL, "klft_batch_set_ptbc: unknown chain %d", chain_ids[r]);
+    if (!b->chains[chain_ids[r]].lat->defect.active)
+      return fail(KLFT_EINVAL, "klft_batch_set_ptbc: chain %d has no defect (klft_lattice_set_defect)", chain_ids[r]);
+  }
+  b->reps.assign(chain_ids, chain_ids + nrep);
+  b->c_of_label.assign(c_of_label, c_of_label + nrep);
+  b->ptbc_beta = beta;
+  b->swap_seed = swap_seed;
+  for (void **p : {(void **)&b->d_c_of_label, (void **)&b->d_c_of_rep, (void **)&b->d_A, (void **)&b->d_part,
+                   (void **)&b->d_label_of_rep, (void **)&b->d_rep_of_label, (void **)&b->d_swap_acc})
+    if (*p) {
+      cudaFree(*p);
+      *p = nullptr;
+    }
+  int maxblk = 1;
+  for (int r = 0; r < nrep; ++r) {
+    const int nb = defect_sums_blocks(b->chains[chain_ids[r]].lat->g);
+    maxblk = nb > maxblk ? nb : maxblk;
+  }
+  CK(cudaMalloc(&b->d_c_of_label, nrep * sizeof(double)));
+  CK(cudaMalloc(&b->d_c_of_rep, nrep * sizeof(double)));
+  CK(cudaMalloc(&b->d_A, 2 * nrep * sizeof(double)));
+  CK(cudaMalloc(&b->d_part, 2 * (size_t)maxblk * sizeof(double)));
+  CK(cudaMalloc(&b->d_label_of_rep, nrep * sizeof(int)));
+  CK(cudaMalloc(&b->d_rep_of_label, nrep * sizeof(int)));
+  CK(cudaMalloc(&b->d_swap_acc, nrep * sizeof(unsigned long long)));
+  std::vector<int> lab(nrep);
+  for (int r = 0; r < nrep; ++r) lab[r] = r;
+  CK(cudaMemcpyAsync(b->d_c_of_label, c_of_label, nrep * sizeof(double), cudaMemcpyHostToDevice, b->stream));
+  CK(cudaMemcpyAsync(b->d_c_of_rep, c_of_label, nrep * sizeof(double), cudaMemcpyHostToDevice, b->stream));
+  CK(cudaMemcpyAsync(b->d_label_of_rep, lab.data(), nrep * sizeof(int), cudaMemcpyHostToDevice, b->stream));
+  CK(cudaMemcpyAsync(b->d_rep_of_label, lab.data(), nrep * sizeof(int), cudaMemcpyHostToDevice, b->stream));
+  CK(cudaMemsetAsync(b->d_swap_acc, 0, nrep * sizeof(unsigned long long), b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  b->dirty = true;
+  return KLFT_OK;
+}
+
+klft_status klft_batch_run(klft_batch *b, int ncycles, int measure_plaquette, int use_graph, double *acc_out,
+                           double *plaq_out, int *labels_out, double *device_ms) {
+  if (!b) return fail(KLFT_EINVAL, "klft_batch_run: null handle");
+  if (ncycles < 0) return fail(KLFT_EINVAL, "klft_batch_run: negative count");
+  if (b->chains.empty()) return fail(KLFT_EINVAL, "klft_batch_run: no chains");
+  if (ncycles == 0) return KLFT_OK;
+  std::lock_guard<std::mutex> guard(b->mtx);
+  const int n = (int)b->chains.size();
+  const int nrep = (int)b->reps.size();
+  // member lattices must be idle: their own streams may still hold work
+  for (auto &ch : b->chains) CK(cudaStreamSynchronize(ch.lat->stream));
+  klft_status s = prepare(b, ncycles);
+  if (s != KLFT_OK) return s;
+  if (b->dirty || b->graph_measure != measure_plaquette) b->drop_graph();
+  CK(cudaMemsetAsync(b->d_slot, 0, sizeof(uint32_t), b->stream));
+  CK(cudaMemsetAsync(b->s_nacc.ptr, 0, (size_t)ncycles * n * sizeof(unsigned long long), b->stream));
+  if (use_graph && !b->exec) {
+    CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    s = enqueue_cycle(b, measure_plaquette);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(b->stream, &graph);
+    if (s != KLFT_OK) {
+      if (graph) cudaGraphDestroy(graph);
+      return s;
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+    b->graph = graph;
+    CK(cudaGraphInstantiate(&b->exec, graph, 0));
+    b->graph_measure = measure_plaquette;
+    b->dirty = false;
+  }
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  CK(cudaEventRecord(e0, b->stream));
+  for (int c = 0; c < ncycles; ++c) {
+    if (use_graph) {
+      CK(cudaGraphLaunch(b->exec, b->stream));
+    } else {
+      s = enqueue_cycle(b, measure_plaquette);
+      if (s != KLFT_OK) return s;
+    }
+  }
+  CK(cudaEventRecord(e1, b->stream));
+  std::vector<unsigned long long> h_nacc((size_t)ncycles * n);
+  CK(cudaMemcpyAsync(h_nacc.data(), b->s_nacc.ptr, h_nacc.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                     b->stream));
+  if (plaq_out && measure_plaquette)
+    CK(cudaMemcpyAsync(plaq_out, b->s_plaq.ptr, (size_t)ncycles * n * sizeof(double), cudaMemcpyDeviceToHost,
+                       b->stream));
+  if (labels_out && nrep > 0)
+    CK(cudaMemcpyAsync(labels_out, b->s_labels.ptr, (size_t)ncycles * nrep * sizeof(int), cudaMemcpyDeviceToHost,
+                       b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (device_ms) *device_ms = ms;
+  for (int i = 0; i < n; ++i) {
+    klft_lattice *lat = b->chains[i].lat;
+    double norm = 1.0;
+    for (int d = 0; d < lat->g.nd; ++d) norm *= (double)lat->g.L[d];
+    norm *= (double)lat->g.nd;
+    norm *= (double)b->chains[i].nhits;
+    for (int c = 0; c < ncycles; ++c) {
+      if (acc_out) acc_out[(size_t)c * n + i] = b->chains[i].nhits ? (double)h_nacc[(size_t)c * n + i] / norm : 0.0;
+      if (plaq_out && measure_plaquette) plaq_out[(size_t)c * n + i] = normalize_plaquette(lat, plaq_out[(size_t)c * n + i]);
+    }
+  }
+  // the replicas' host-side defect coefficients follow the device labels
+  if (nrep > 0) {
+    std::vector<double> crep(nrep);
+    CK(cudaMemcpy(crep.data(), b->d_c_of_rep, nrep * sizeof(double), cudaMemcpyDeviceToHost));
+    for (int r = 0; r < nrep; ++r) b->chains[b->reps[r]].lat->defect.c = crep[r];
+  }
+  return KLFT_OK;
+}
+
+klft_status klft_batch_swap_stats(klft_batch *b, unsigned long long *accepted_per_pair) {
+  if (!b || !accepted_per_pair) return fail(KLFT_EINVAL, "klft_batch_swap_stats: null pointer");
+  std::lock_guard<std::mutex> guard(b->mtx);
+  const int nrep = (int)b->reps.size();
+  if (nrep == 0) return KLFT_OK;
+  CK(cudaMemcpy(accepted_per_pair, b->d_swap_acc, (size_t)(nrep - 1 > 0 ? nrep - 1 : 0) * sizeof(unsigned long long),
+                cudaMemcpyDeviceToHost));
+  return KLFT_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,213 @@
+// metropolis_site.cuh -- the per-site Metropolis update shared by the
+// single-lattice pass kernels (metropolis.cu) and the multi-chain batch kernels
+// (batch.cu).
+//
+// Semantics follow MetropolisGaugeField::operator() (Metropolis.hpp:73-113): a
+// thread owns one site of a parity class and updates its Nd links in order
+// mu = 0..Nd-1; per link the staple is formed once, then nHits proposals
+// U' = U r are accepted with probability min(1, exp(-dS)),
+// dS = -(beta/Nc) Re Tr[(U' - U) S], and an accepted link is stored
+// reunitarised (restoreSUN).
+//
+// Per-hit cost is cut by carrying M = S U: Re Tr(U r S) = Re Tr(r M) needs only
+// the diagonal of r M (36 flops for SU(3)) instead of the product U r; U r and M
+// are rebuilt only on acceptance.
+//
+// Random numbers: the reference proposals (U(1), SU(2), the SU(3)
+// Gram-Schmidt generator) consume the site's sequential Philox stream in the
+// order the reference functor consumes its generator.  The exp(i eps H)
+// proposal (no reference counterpart) reads fixed stream positions per hit (see
+// ExpHitStream), so a proposal does not depend on earlier accept decisions.
+// Neither depends on the launch shape.
+#pragma once
+#include "group.cuh"
+#include "kernels.cuh"
+#include "staple.cuh"
+
+namespace klft {
+
+// Fixed-position stream of the exp(i eps H) proposal: hit h of a site
+// (h = mu*nHits + hit) uses Philox blocks 3h, 3h+1 (eight 32-bit uniforms
+// u = (w + 1/2) 2^-32 for four Box-Muller pairs) and 3h+2 (53-bit accept
+// uniform) of the (sweep, site) counter.
+struct ExpHitStream {
+  uint32_t k0, k1, site, step;
+  KLFT_D void block(uint32_t b, uint32_t w[4]) const {
+    w[0] = b; w[1] = site; w[2] = step; w[3] = KIND_METROPOLIS << 24;
+    philox4x32_10(w, k0, k1);
+  }
+  KLFT_D double accept_uniform(uint32_t h) const {
+    uint32_t w[4];
+    block(3 * h + 2, w);
+    return (double)((((uint64_t)w[0] << 32) | w[1]) >> 11) * 0x1.0p-53;
+  }
+};
+
+KLFT_D void box_muller(uint32_t wa, uint32_t wb, double &g0, double &g1) {
+  const double ua = ((double)wa + 0.5) * 0x1.0p-32, ub = ((double)wb + 0.5) * 0x1.0p-32;
+  const double r = sqrt(-2.0 * log(ua));
+  double s, c;
+  sincospi(2.0 * ub, &s, &c);
+  g0 = r * c;
+  g1 = r * s;
+}
+// Mixed form: SFU log and sincos.  cos/sin(2 pi u) = -cos/sin(2 pi (u - 1/2)) keeps
+// the SFU argument in [-pi, pi].
+KLFT_D void box_muller(uint32_t wa, uint32_t wb, float &g0, float &g1) {
+  const float ua = fmaf((float)wa, 0x1.0p-32f, 0x1.0p-33f), ub = fmaf((float)wb, 0x1.0p-32f, 0x1.0p-33f);
+  const float r = sqrtf(-2.0f * __logf(ua));
+  float s, c;
+  __sincosf(6.28318530717958648f * (ub - 0.5f), &s, &c);
+  g0 = -r * c;
+  g1 = -r * s;
+}
+
+template <typename T>
+KLFT_D Mat<3, T> exp_proposal(const ExpHitStream &hs, uint32_t h, T half_eps) {
+  uint32_t w[8];
+  hs.block(3 * h, w);
+  hs.block(3 * h + 1, w + 4);
+  T g[8];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) box_muller(w[2 * k], w[2 * k + 1], g[2 * k], g[2 * k + 1]);
+  return expi_su3(gellmann_combo(g, half_eps));
+}
+
+template <int NC, typename T>
+KLFT_D T retr_diag(const Mat<NC, T> &M) {
+  T t = T(0);
+#pragma unroll
+  for (int i = 0; i < NC; ++i) t += M.e[i][i].re;
+  return t;
+}
+
+// Block total of accepted hits -> one atomic per block.
+KLFT_D void add_accepts(int nacc, unsigned long long *d_nacc) {
+  __shared__ int red[32];
+  const int v = warp_sum(nacc);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int s = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
+    if (s) atomicAdd(d_nacc, (unsigned long long)s);
+  }
+}
+
+// site t of parity class val: x_d = 2 h_d + bit_d, bit_d = (val >> (Nd-1-d)) & 1
+KLFT_D Site pass_site(const Geom &g, long long t, int val, int nd) {
+  Site x;
+#pragma unroll
+  for (int d = 0; d < 4; ++d) {
+    x.h[d] = (int)(t % g.H[d]);
+    t /= g.H[d];
+    x.b[d] = d < nd ? (val >> (nd - 1 - d)) & 1 : 0;
+  }
+  return x;
+}
+
+template <typename T> struct MinBlocks { static constexpr int v = 4; };
+template <> struct MinBlocks<double> { static constexpr int v = 2; };
+
+// Reference proposals: sequential per-site stream, exactly as the reference consumes it.
+template <int NC, int ND, typename T, bool DF>
+KLFT_D int site_update_ref(const Links<NC, T> &U, const Geom &g, const Site &x, const MetroArgs &a, uint32_t sweep,
+                           const Defect &df) {
+  int nacc = 0;
+  Stream rng(a.seed, a.chain, site_lex(g, x), sweep, KIND_METROPOLIS, 0);
+  const long long lx = site_lin(g, x);
+  const T bnc = (T)a.beta / (T)NC;
+#pragma unroll 1
+  for (int mu = 0; mu < ND; ++mu) {
+    const Mat<NC, T> S = staple<NC, ND, T, DF>(U, g, x, mu, df);
+    const bool dlink = DF && df.active && in_defect(g, df, x, mu);
+    Mat<NC, T> Uo = U.load(lx, mu);
+    Mat<NC, T> M = mul(S, Uo);
+    T trO = retr_diag(M);
+    bool changed = false;
+#pragma unroll 1
+    for (int hit = 0; hit < a.nhits; ++hit) {
+      const Mat<NC, T> rr = propose<T>(rng, (const Mat<NC, T> *)nullptr, a.delta, PROPOSAL_REFERENCE, 0.0);
+      T dS = -bnc * (retr_mul(rr, M) - trO);
+      if (dlink) dS *= (T)defect_c(df);
+      bool accept = dS < T(0);
+      if (!accept) accept = rng.next() < (double)exp(-dS);
+      if (accept) {
+        Uo = restore(mul(Uo, rr));
+        M = mul(S, Uo);
+        trO = retr_diag(M);
+        ++nacc;
+        changed = true;
+      }
+    }
+    if (changed) U.store(lx, mu, Uo);
+  }
+  return nacc;
+}
+
+// SU(3) exp(i eps H) proposals at fixed stream positions.  Staple and link wait
+// in shared memory (read only on acceptance: M = S U), one structure-of-arrays
+// slot per thread, leaving registers to the proposal.
+template <int ND, typename T, bool DF>
+KLFT_D int site_update_exp(const Links<3, T> &U, const Geom &g, const Site &x, const MetroArgs &a, uint32_t sweep,
+                           const Defect &df) {
+  __shared__ cx<T> s_S[9][128];
+  __shared__ cx<T> s_U[9][128];
+  const int tid = threadIdx.x;
+  int nacc = 0;
+  const ExpHitStream hs{(uint32_t)a.seed, (uint32_t)(a.seed >> 32) ^ (uint32_t)a.chain, site_lex(g, x), sweep};
+  const long long lx = site_lin(g, x);
+  const T bnc = (T)a.beta / T(3);
+  const T half_eps = (T)(0.5 * a.eps);
+#pragma unroll 1
+  for (int mu = 0; mu < ND; ++mu) {
+    const uint32_t h0 = (uint32_t)(mu * a.nhits);
+    Mat<3, T> M;
+    {
+      const Mat<3, T> Uo = U.load(lx, mu);
+      const Mat<3, T> S = staple<3, ND, T, DF>(U, g, x, mu, df);
+#pragma unroll
+      for (int k = 0; k < 9; ++k) {
+        s_S[k][tid] = S.e[k / 3][k % 3];
+        s_U[k][tid] = Uo.e[k / 3][k % 3];
+      }
+      M = mul(S, Uo);
+    }
+    Mat<3, T> rr;
+    const bool dlink = DF && df.active && in_defect(g, df, x, mu);
+    T trO = retr_diag(M);
+    bool changed = false;
+#pragma unroll 1
+    for (int hit = 0; hit < a.nhits; ++hit) {
+      rr = exp_proposal<T>(hs, h0 + hit, half_eps);
+      T dS = -bnc * (retr_mul(rr, M) - trO);
+      if (dlink) dS *= (T)defect_c(df);
+      bool accept = dS < T(0);
+      if (!accept) accept = hs.accept_uniform(h0 + hit) < (double)exp(-dS);
+      if (accept) {
+        Mat<3, T> Uo, S;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) Uo.e[k / 3][k % 3] = s_U[k][tid];
+        Uo = restore(mul(Uo, rr));
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+          s_U[k][tid] = Uo.e[k / 3][k % 3];
+          S.e[k / 3][k % 3] = s_S[k][tid];
+        }
+        M = mul(S, Uo);
+        trO = retr_diag(M);
+        ++nacc;
+        changed = true;
+      }
+    }
+    if (changed) {
+      Mat<3, T> Uo;
+#pragma unroll
+      for (int k = 0; k < 9; ++k) Uo.e[k / 3][k % 3] = s_U[k][tid];
+      U.store(lx, mu, Uo);
+    }
+  }
+  return nacc;
+}
+
+}  // namespace klft

@@ -8,16 +8,19 @@
 
 namespace klft {
 
-template <int NC, typename T>
+// DF = false compiles the defect handling out (lattices without a PTBC defect).
+template <int NC, typename T, bool DF>
 KLFT_D Mat<NC, T> load_link(const Links<NC, T> &U, const Geom &g, const Site &s, int mu, const Defect &df) {
   Mat<NC, T> m = U.load(site_lin(g, s), mu);
-  if (df.active && in_defect(g, df, s, mu)) m = mscale(m, (T)defect_c(df));
+  if constexpr (DF) {
+    if (df.active && in_defect(g, df, s, mu)) m = mscale(m, (T)defect_c(df));
+  }
   return m;
 }
 
 // The nu loops stay rolled: the update kernels are instruction-fetch bound when
 // the 4(Nd-1) products are all inlined next to the proposal code.
-template <int NC, int ND, typename T>
+template <int NC, int ND, typename T, bool DF = false>
 KLFT_D Mat<NC, T> staple(const Links<NC, T> &U, const Geom &g, const Site &x, int mu, const Defect &df) {
   Mat<NC, T> S = mzero<NC, T>();
   const Site xpmu = site_up(g, x, mu);
@@ -25,16 +28,16 @@ KLFT_D Mat<NC, T> staple(const Links<NC, T> &U, const Geom &g, const Site &x, in
   for (int nu = 0; nu < ND; ++nu) {
     if (nu == mu) continue;
     const Site xpnu = site_up(g, x, nu);
-    const Mat<NC, T> t = mul_nd(load_link(U, g, xpmu, nu, df), load_link(U, g, xpnu, mu, df));
-    madd(S, mul_nd(t, load_link(U, g, x, nu, df)));
+    const Mat<NC, T> t = mul_nd(load_link<NC, T, DF>(U,g, xpmu, nu, df), load_link<NC, T, DF>(U,g, xpnu, mu, df));
+    madd(S, mul_nd(t, load_link<NC, T, DF>(U,g, x, nu, df)));
   }
 #pragma unroll 1
   for (int nu = 0; nu < ND; ++nu) {
     if (nu == mu) continue;
     const Site xpmu_mnu = site_dn(g, xpmu, nu);
     const Site xmnu = site_dn(g, x, nu);
-    const Mat<NC, T> t = mul_dd(load_link(U, g, xpmu_mnu, nu, df), load_link(U, g, xmnu, mu, df));
-    madd(S, mul(t, load_link(U, g, xmnu, nu, df)));
+    const Mat<NC, T> t = mul_dd(load_link<NC, T, DF>(U,g, xpmu_mnu, nu, df), load_link<NC, T, DF>(U,g, xmnu, mu, df));
+    madd(S, mul(t, load_link<NC, T, DF>(U,g, xmnu, nu, df)));
   }
   return S;
 }
