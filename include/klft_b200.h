@@ -30,7 +30,10 @@ typedef enum {
   KLFT_ENOMEM = 2,   /* device or host allocation failed    */
   KLFT_ECUDA = 3,    /* CUDA runtime error / no device      */
   KLFT_ETIMEOUT = 4, /* a bounded device wait gave up       */
-  KLFT_ENOTSUP = 5   /* combination not supported           */
+  KLFT_ENOTSUP = 5,  /* combination not supported           */
+  KLFT_ECANCELED = 6, /* serving: the job was cancelled     */
+  KLFT_EINTERNAL = 7, /* serving: the worker failed          */
+  KLFT_EBUSY = 8      /* serving: admission queue is full    */
 } klft_status;
 
 typedef enum { KLFT_PRECISION_FP64 = 0, KLFT_PRECISION_MIXED = 1 } klft_precision;
@@ -182,6 +185,91 @@ klft_status klft_tuner_write_cache(const char *path);
 /* values[0..rank-1] of a cached key; *rank = 0 when absent. */
 klft_status klft_tuner_lookup(const char *key, int *values, int *rank);
 klft_status klft_tuner_clear(void);
+
+/* ---------------------------------------------------------------- serving
+ * No counterpart in the reference (its only drivers are the metropolis and hmc
+ * binaries, Metropolis.hpp:113-223 and HMC.hpp:20-117, one run per process).
+ * A server owns one worker thread on one GPU.  Jobs are queued by
+ * klft_server_submit and admitted in arrival order while their device
+ * footprint (klft_job_footprint) fits the memory budget and fewer than
+ * max_active jobs run.  Admitted jobs keep their lattice and RNG counters
+ * resident until they finish.  Metropolis jobs advance together: every round
+ * sweeps each running job once per step in multi-chain launches (one per
+ * parity class and group of lattices of one kind), so jobs that arrive while
+ * others run join the next round.  HMC jobs run trajectories on their own
+ * streams beside the rounds.  A finished job is measured on its final
+ * configuration (plaquette, temporal Wilson loops) and its result is posted
+ * for klft_server_poll.  A job's result depends only on its description: it
+ * is the same, bit for bit, alone and in any mix. */
+typedef enum { KLFT_JOB_METROPOLIS = 0, KLFT_JOB_HMC = 1 } klft_job_kind;
+#define KLFT_JOB_MAX_WILSON 16
+typedef struct klft_job {
+  int kind;      /* klft_job_kind */
+  int nc, ndims; /* group U(1)/SU(2)/SU(3), 2..4 dims */
+  int L[4];      /* even extents */
+  int precision, start;
+  uint64_t seed, chain; /* Philox stream of the job */
+  double beta;
+  /* Metropolis (klft_metropolis_sweeps) */
+  int nsweeps, nhits, proposal;
+  double delta, eps;
+  /* HMC (klft_hmc_trajectories) */
+  int ntraj, nsteps, integrator;
+  double tau;
+  /* measurements of the final configuration */
+  int measure_plaquette;
+  int n_wilson;                            /* temporal loops, <= KLFT_JOB_MAX_WILSON */
+  int wilson_pairs[2 * KLFT_JOB_MAX_WILSON]; /* (L, T) pairs */
+} klft_job;
+
+typedef struct klft_job_result {
+  uint64_t id;
+  int status;                        /* KLFT_OK or why the job failed */
+  int kind;
+  double plaquette;                  /* NaN unless measured */
+  double wilson[KLFT_JOB_MAX_WILSON]; /* W_temp of the requested pairs */
+  double acceptance;                 /* accepted hits / proposals, or accepted trajectories / ntraj */
+  double mean_exp_mdH;               /* HMC: <exp(-dH)>; NaN for Metropolis */
+  double mean_dH;                    /* HMC: <dH> */
+  unsigned long long link_updates;   /* links visited: sweeps * V * Nd, or integrator link updates */
+  double t_submit, t_admit, t_finish; /* seconds on the server's steady clock */
+  char error[160];
+} klft_job_result;
+
+typedef struct klft_server_stats {
+  unsigned long long submitted, completed, failed, cancelled, rejected;
+  int queued, active;
+  uint64_t bytes_in_use, bytes_budget;
+  unsigned long long link_updates; /* of completed jobs */
+  unsigned long long rounds;       /* Metropolis rounds enqueued */
+  unsigned long long launches;     /* kernels the worker launched */
+  double busy_s;                   /* seconds with at least one job admitted */
+} klft_server_stats;
+
+typedef struct klft_server klft_server;
+/* device: CUDA ordinal.  budget_bytes: device memory the jobs may hold (0: 90%
+ * of the free memory at creation).  max_active: running jobs (0: 256).
+ * max_queued: waiting jobs before submit answers KLFT_EBUSY (0: 4096). */
+klft_status klft_server_create(int device, uint64_t budget_bytes, int max_active, int max_queued,
+                               klft_server **out);
+/* Stops the worker after the GPU work in flight; unpolled results are dropped. */
+klft_status klft_server_destroy(klft_server *s);
+/* Device bytes a job holds while admitted. */
+klft_status klft_job_footprint(const klft_job *job, uint64_t *bytes);
+/* KLFT_EINVAL: malformed job; KLFT_ENOMEM: footprint above the budget (never
+ * admissible); KLFT_EBUSY: queue full.  *id identifies the job's result. */
+klft_status klft_server_submit(klft_server *s, const klft_job *job, uint64_t *id);
+/* A queued job is dropped, a running one stops after its work in flight; both
+ * post a result with status KLFT_ECANCELED.  KLFT_EINVAL for unknown or
+ * finished ids. */
+klft_status klft_server_cancel(klft_server *s, uint64_t id);
+/* Up to max finished results, in completion order; waits up to timeout_ms for
+ * the first one (0: no wait). */
+klft_status klft_server_poll(klft_server *s, klft_job_result *out, int max, int timeout_ms, int *n);
+klft_status klft_server_stats_get(klft_server *s, klft_server_stats *st);
+/* Host-side fault injection for tests: 1 = the worker throws at its next
+ * iteration (running jobs fail with KLFT_EINTERNAL, the worker carries on). */
+klft_status klft_server_inject_fault(klft_server *s, int what);
 
 /* No counterpart in the reference.  klft_metropolis_sweeps without any
  * allocation, for callers that cannot let the library allocate when they sweep:

@@ -31,7 +31,7 @@ INTEGRATOR = {"reference": 0, "leapfrog": 1, "omelyan": 2}
 __all__ = [
     "GaugeField", "MetropolisParams", "GaugeObservableParams", "KlftError", "sweep_Metropolis",
     "run_metropolis", "GaugePlaquette", "WilsonLoop_mu_nu", "WilsonLoop_temporal",
-    "measureGaugeObservables", "flushAllGaugeObservables", "device_count",
+    "measureGaugeObservables", "flushAllGaugeObservables", "device_count", "Server", "JobSpec",
 ]
 
 
@@ -414,3 +414,6 @@ def run_metropolis(g: GaugeField, mp: MetropolisParams, op: GaugeObservableParam
         measureGaugeObservables(g, op, step)
     flushAllGaugeObservables(op)
     return 0
+
+
+from .serve import JobSpec, Server  # noqa: E402

@@ -17,6 +17,37 @@ _u32p = C.POINTER(C.c_uint32)
 _llp = C.POINTER(C.c_longlong)
 _vp = C.c_void_p
 
+JOB_MAX_WILSON = 16
+
+
+class Job(C.Structure):
+    """struct klft_job (include/klft_b200.h)."""
+    _fields_ = [("kind", C.c_int), ("nc", C.c_int), ("ndims", C.c_int), ("L", C.c_int * 4),
+                ("precision", C.c_int), ("start", C.c_int), ("seed", C.c_uint64), ("chain", C.c_uint64),
+                ("beta", C.c_double), ("nsweeps", C.c_int), ("nhits", C.c_int), ("proposal", C.c_int),
+                ("delta", C.c_double), ("eps", C.c_double), ("ntraj", C.c_int), ("nsteps", C.c_int),
+                ("integrator", C.c_int), ("tau", C.c_double), ("measure_plaquette", C.c_int),
+                ("n_wilson", C.c_int), ("wilson_pairs", C.c_int * (2 * JOB_MAX_WILSON))]
+
+
+class JobResult(C.Structure):
+    """struct klft_job_result."""
+    _fields_ = [("id", C.c_uint64), ("status", C.c_int), ("kind", C.c_int), ("plaquette", C.c_double),
+                ("wilson", C.c_double * JOB_MAX_WILSON), ("acceptance", C.c_double),
+                ("mean_exp_mdH", C.c_double), ("mean_dH", C.c_double), ("link_updates", C.c_ulonglong),
+                ("t_submit", C.c_double), ("t_admit", C.c_double), ("t_finish", C.c_double),
+                ("error", C.c_char * 160)]
+
+
+class ServerStats(C.Structure):
+    """struct klft_server_stats."""
+    _fields_ = [("submitted", C.c_ulonglong), ("completed", C.c_ulonglong), ("failed", C.c_ulonglong),
+                ("cancelled", C.c_ulonglong), ("rejected", C.c_ulonglong), ("queued", C.c_int),
+                ("active", C.c_int), ("bytes_in_use", C.c_uint64), ("bytes_budget", C.c_uint64),
+                ("link_updates", C.c_ulonglong), ("rounds", C.c_ulonglong), ("launches", C.c_ulonglong),
+                ("busy_s", C.c_double)]
+
+
 # name -> (restype, argtypes); every symbol declared in include/klft_b200.h
 SIGNATURES = {
     "klft_last_error": (C.c_char_p, []),
@@ -61,11 +92,20 @@ SIGNATURES = {
     "klft_tuner_clear": (C.c_int, []),
     "klft_ptbc_defect_sums": (C.c_int, [_vp, C.c_double, _dp]),
     "klft_ptbc_swap": (C.c_int, [C.POINTER(_vp), C.c_int, _dp, _ip, C.c_double, C.c_uint64, C.c_uint32, _ip]),
+    "klft_job_footprint": (C.c_int, [C.POINTER(Job), C.POINTER(C.c_uint64)]),
+    "klft_server_create": (C.c_int, [C.c_int, C.c_uint64, C.c_int, C.c_int, C.POINTER(_vp)]),
+    "klft_server_destroy": (C.c_int, [_vp]),
+    "klft_server_submit": (C.c_int, [_vp, C.POINTER(Job), C.POINTER(C.c_uint64)]),
+    "klft_server_cancel": (C.c_int, [_vp, C.c_uint64]),
+    "klft_server_poll": (C.c_int, [_vp, C.POINTER(JobResult), C.c_int, C.c_int, _ip]),
+    "klft_server_stats_get": (C.c_int, [_vp, C.POINTER(ServerStats)]),
+    "klft_server_inject_fault": (C.c_int, [_vp, C.c_int]),
     "klft_metropolis_sweeps_noalloc": (C.c_int, [_vp, C.c_double, C.c_double, C.c_int, C.c_int, C.c_double, C.c_int,
                                                  _dp]),
 }
 
-STATUS = {0: "KLFT_OK", 1: "KLFT_EINVAL", 2: "KLFT_ENOMEM", 3: "KLFT_ECUDA", 4: "KLFT_ETIMEOUT", 5: "KLFT_ENOTSUP"}
+STATUS = {0: "KLFT_OK", 1: "KLFT_EINVAL", 2: "KLFT_ENOMEM", 3: "KLFT_ECUDA", 4: "KLFT_ETIMEOUT", 5: "KLFT_ENOTSUP",
+          6: "KLFT_ECANCELED", 7: "KLFT_EINTERNAL", 8: "KLFT_EBUSY"}
 
 
 class KlftError(RuntimeError):

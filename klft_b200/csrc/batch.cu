@@ -14,6 +14,7 @@
 // device counter, so the captured graph is replayed unchanged.  Replica swaps
 // run on the device (ptbc.cu) and write each replica's defect coefficient,
 // which the sweep kernels read through Defect::dyn_c.
+#include <algorithm>
 #include <cstring>
 #include <memory>
 #include <vector>
@@ -73,6 +74,17 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::v)
 __global__ void batch_advance_kernel(uint32_t *const *ctrs, int n) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) ctrs[i][0] += 1u;
+}
+
+// sweep counters of up to CtrList::MAX lattices, passed by value
+struct CtrList {
+  static constexpr int MAX = 128;
+  int n;
+  uint32_t *p[MAX];
+};
+
+__global__ void advance_list_kernel(const __grid_constant__ CtrList l) {
+  if ((int)threadIdx.x < l.n) l.p[threadIdx.x][0] += 1u;
 }
 
 __global__ void batch_slot_kernel(uint32_t *slot, uint32_t *cycle) {
@@ -196,20 +208,24 @@ struct Group {
   std::vector<int> blocks;
 };
 
-// Enqueue one cycle on b->stream (recorded into the graph by the caller).
-klft_status enqueue_cycle(klft_batch *b, int measure) {
-  const int n = (int)b->chains.size();
+}  // namespace
+
+namespace klft {
+
+// One sweep of every item, interleaved by parity class, in multi-chain launches
+// on stream st.  Accepted hits of item i go to nacc[(*slot) * stride + index],
+// index = items[i].acc_index (i when negative), stride = acc_stride (n when 0);
+// the caller advances the items' sweep counters afterwards.
+klft_status enqueue_multi_sweep(const std::vector<SweepItem> &items, unsigned long long *nacc, const uint32_t *slot,
+                                cudaStream_t st, int acc_stride, int *nlaunch) {
+  const int n = (int)items.size();
+  const int stride = acc_stride > 0 ? acc_stride : n;
   std::vector<Group> groups;
-  int replica_of_chain_none = -1;
-  (void)replica_of_chain_none;
   for (int i = 0; i < n; ++i) {
-    const auto &ch = b->chains[i];
-    klft_lattice *lat = ch.lat;
-    int rep = -1;
-    for (size_t r = 0; r < b->reps.size(); ++r)
-      if (b->reps[r] == i) rep = (int)r;
-    GroupKey key{lat->nc, lat->g.nd, lat->dtype(), (lat->nc == 3 && ch.proposal == KLFT_PROPOSAL_EXP) ? 1 : 0,
-                 lat->defect.active ? 1 : 0};
+    const SweepItem &it = items[i];
+    klft_lattice *lat = it.lat;
+    GroupKey key{lat->nc, lat->g.nd, lat->dtype(), (lat->nc == 3 && it.a.proposal == KLFT_PROPOSAL_EXP) ? 1 : 0,
+                 it.df.active ? 1 : 0};
     Group *grp = nullptr;
     for (auto &gg : groups)
       if (gg.key == key) grp = &gg;
@@ -220,7 +236,7 @@ klft_status enqueue_cycle(klft_batch *b, int measure) {
     if (grp->tables.empty() || grp->tables.back()->n == BATCH_MAX) {
       grp->tables.emplace_back(new ChainTable());
       std::memset(grp->tables.back().get(), 0, sizeof(ChainTable));
-      grp->tables.back()->nchains_total = n;
+      grp->tables.back()->nchains_total = stride;
       grp->blocks.push_back(0);
     }
     ChainTable &tab = *grp->tables.back();
@@ -228,24 +244,63 @@ klft_status enqueue_cycle(klft_batch *b, int measure) {
     d.links = lat->links;
     d.ctr = lat->d_counters;
     d.g = lat->g;
-    d.a = MetroArgs{ch.beta, ch.delta, ch.eps, ch.nhits, ch.proposal, lat->seed, lat->chain};
-    d.df = lat->defect;
-    if (rep >= 0) d.df.dyn_c = b->d_c_of_rep + rep;
-    d.index = i;
+    d.a = it.a;
+    d.df = it.df;
+    d.index = it.acc_index >= 0 ? it.acc_index : i;
     d.block_begin = grp->blocks.back();
     grp->blocks.back() += (int)((lat->g.Vh + 127) / 128);
   }
-  unsigned long long *nacc = (unsigned long long *)b->s_nacc.ptr;
   int maxnd = 0;
   for (auto &gg : groups) maxnd = gg.key.nd > maxnd ? gg.key.nd : maxnd;
   for (int val = 0; val < (1 << maxnd); ++val)
     for (auto &gg : groups) {
       if (val >= (1 << gg.key.nd)) continue;
-      for (size_t t = 0; t < gg.tables.size(); ++t)
-        CK(launch_group(gg.key, *gg.tables[t], gg.blocks[t], val, nacc, b->d_slot, b->stream));
+      for (size_t t = 0; t < gg.tables.size(); ++t) {
+        CK(launch_group(gg.key, *gg.tables[t], gg.blocks[t], val, nacc, slot, st));
+        if (nlaunch) ++*nlaunch;
+      }
     }
-  batch_advance_kernel<<<(n + 127) / 128, 128, 0, b->stream>>>(b->d_ctrs, n);
-  CK(cudaGetLastError());
+  return KLFT_OK;
+}
+
+cudaError_t launch_advance_many(uint32_t *const *d_ctrs, int n, cudaStream_t st) {
+  batch_advance_kernel<<<(n + 127) / 128, 128, 0, st>>>(d_ctrs, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_advance_list(const std::vector<uint32_t *> &ctrs, cudaStream_t st, int *nlaunch) {
+  for (size_t b = 0; b < ctrs.size(); b += CtrList::MAX) {
+    CtrList l;
+    l.n = (int)std::min(ctrs.size() - b, (size_t)CtrList::MAX);
+    for (int i = 0; i < l.n; ++i) l.p[i] = ctrs[b + i];
+    advance_list_kernel<<<1, CtrList::MAX, 0, st>>>(l);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    if (nlaunch) ++*nlaunch;
+  }
+  return cudaSuccess;
+}
+
+}  // namespace klft
+
+namespace {
+
+// Enqueue one cycle on b->stream (recorded into the graph by the caller).
+klft_status enqueue_cycle(klft_batch *b, int measure) {
+  const int n = (int)b->chains.size();
+  std::vector<SweepItem> items;
+  for (int i = 0; i < n; ++i) {
+    const auto &ch = b->chains[i];
+    klft_lattice *lat = ch.lat;
+    SweepItem it{lat, MetroArgs{ch.beta, ch.delta, ch.eps, ch.nhits, ch.proposal, lat->seed, lat->chain},
+                 lat->defect, -1};
+    for (size_t r = 0; r < b->reps.size(); ++r)
+      if (b->reps[r] == i) it.df.dyn_c = b->d_c_of_rep + r;
+    items.push_back(it);
+  }
+  klft_status st = enqueue_multi_sweep(items, (unsigned long long *)b->s_nacc.ptr, b->d_slot, b->stream, 0, nullptr);
+  if (st != KLFT_OK) return st;
+  CK(launch_advance_many(b->d_ctrs, n, b->stream));
   if (!b->reps.empty()) {
     const int nrep = (int)b->reps.size();
     for (int r = 0; r < nrep; ++r) {

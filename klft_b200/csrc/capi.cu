@@ -78,6 +78,27 @@ static klft_status check_proposal(const klft_lattice *lat, double delta, int pro
   return KLFT_OK;
 }
 
+namespace klft {
+// extents already checked (even, >= 2, volume < 2^31)
+Geom make_geom(int ndims, const int *L) {
+  Geom g{};
+  g.nd = ndims;
+  long long V = 1, Vh = 1;
+  int stride = 1;
+  for (int d = 0; d < 4; ++d) {
+    g.L[d] = d < ndims ? L[d] : 1;
+    g.H[d] = d < ndims ? L[d] / 2 : 1;
+    g.hs[d] = stride;
+    stride *= g.H[d];
+    Vh *= g.H[d];
+    if (d < ndims) V *= L[d];
+  }
+  g.V = V;
+  g.Vh = Vh;
+  return g;
+}
+}  // namespace klft
+
 extern "C" {
 
 const char *klft_last_error(void) { return g_last_error.c_str(); }
@@ -120,20 +141,8 @@ klft_status klft_lattice_create(int nc, int ndims, const int *L, int precision, 
   lat->precision = precision;
   lat->seed = seed;
   lat->chain = 0;
-  Geom &g = lat->g;
-  g.nd = ndims;
-  long long Vh = 1;
-  int stride = 1;
-  for (int d = 0; d < 4; ++d) {
-    g.L[d] = d < ndims ? L[d] : 1;
-    g.H[d] = d < ndims ? L[d] / 2 : 1;
-    g.hs[d] = stride;
-    stride *= g.H[d];
-    Vh *= g.H[d];
-  }
-  g.V = V;
-  g.Vh = Vh;
-  // lattices with a singleton parity dimension keep the 2-class structure per dim
+  lat->g = make_geom(ndims, L);
+  const Geom &g = lat->g;
   cudaGetDevice(&lat->device);
   lat->link_bytes = (size_t)V * ndims * nc * nc * elem_bytes(precision);
   e = cudaStreamCreateWithFlags(&lat->stream, cudaStreamNonBlocking);

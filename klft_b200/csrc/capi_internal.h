@@ -4,9 +4,11 @@
 #include <cuda_runtime.h>
 
 #include <mutex>
+#include <vector>
 
 #include "../../include/klft_b200.h"
 #include "common.cuh"
+#include "kernels.cuh"
 
 #define KLFT_RESULT_SLOTS 256
 
@@ -37,6 +39,7 @@ struct klft_lattice {
   uint32_t *d_counters = nullptr;  // [0] sweep, [1] trajectory, [2] cycle
   double *h_results = nullptr;     // pinned, KLFT_RESULT_SLOTS doubles
   klft::Scratch s_part, s_out, s_aux, s_stage, s_wl, s_hmc, s_gf, s_tab, s_tune;
+  int hmc_cap = 0;  // trajectories the HMC buffers in s_hmc are laid out for
   klft::Defect defect{0, 1, {0, 0, 0}, 1.0, nullptr};
   std::mutex mtx;
   int dtype() const { return precision == KLFT_PRECISION_FP64 ? 0 : 1; }
@@ -44,12 +47,35 @@ struct klft_lattice {
 
 namespace klft {
 klft_status lattice_sync(klft_lattice *lat);
+Geom make_geom(int ndims, const int *L);
 // may_tune = false: use only tuned values already known (no timing, no scratch)
 klft_status enqueue_sweeps(klft_lattice *lat, double beta, double delta, int nhits, int proposal, double eps,
                            int nsweeps, unsigned long long *d_nacc, const Defect &df, bool may_tune = true);
 klft_status enqueue_plaquette(klft_lattice *lat, int slot);
 double normalize_plaquette(const klft_lattice *lat, double sum);
 double normalize_wilson(const klft_lattice *lat, double sum);
+// One lattice's share of a multi-chain sweep (batch.cu).
+struct SweepItem {
+  klft_lattice *lat;
+  MetroArgs a;
+  Defect df;
+  int acc_index;  // accept-counter index; < 0: the item's position
+};
+klft_status enqueue_multi_sweep(const std::vector<SweepItem> &items, unsigned long long *nacc, const uint32_t *slot,
+                                cudaStream_t st, int acc_stride, int *nlaunch);
+// sweep counters += 1: a device array of counter pointers, or a host list
+cudaError_t launch_advance_many(uint32_t *const *d_ctrs, int n, cudaStream_t st);
+cudaError_t launch_advance_list(const std::vector<uint32_t *> &ctrs, cudaStream_t st, int *nlaunch);
+// HMC pieces on the lattice's stream (hmc.cu).  hmc_prepare sizes every buffer
+// for ntraj trajectories (it may allocate; nothing else below does).
+klft_status hmc_prepare(klft_lattice *lat, int ntraj);
+// trajectory k (< ntraj of hmc_prepare): momenta, H, integrate, H', accept/restore
+klft_status hmc_enqueue_trajectory(klft_lattice *lat, double beta, double tau, int nsteps, int integrator, int k);
+// d_out[0] = accepted trajectories, d_out[1] = sum exp(-dH), d_out[2] = sum dH over the first ntraj
+klft_status hmc_enqueue_summary(klft_lattice *lat, int ntraj, double *d_out);
+// device bytes of the HMC buffers for ntraj trajectories
+size_t hmc_footprint(int nc, int dtype, const Geom &g, int ntraj);
+
 // Device tables of a Wilson-loop pair list (offsets are int indices into s_tab).
 struct WilsonPlan {
   int npairs = 0, lmax = 0, tmax = 0;

@@ -210,11 +210,15 @@ size_t p_bytes(const klft_lattice *lat) {
   return (size_t)lat->g.V * lat->g.nd * ncomp_of(lat->nc) * (lat->dtype() == 0 ? 8 : 4);
 }
 
+// The layout depends on the trajectory capacity kept in the handle, which only
+// grows, so buffers sized once for ntraj keep their places for every k < ntraj.
 klft_status hmc_bufs(klft_lattice *lat, int ntraj, HmcBufs &b) {
   auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+  if (ntraj < lat->hmc_cap) ntraj = lat->hmc_cap;
   const size_t pb = al(p_bytes(lat)), lb = al(lat->link_bytes);
   const size_t need = pb + lb + al(8 * sizeof(double)) + al((size_t)ntraj * sizeof(double)) + al((size_t)ntraj * sizeof(int));
   CK(lat->s_hmc.ensure(need));
+  lat->hmc_cap = ntraj;
   char *base = (char *)lat->s_hmc.ptr;
   b.P = base;
   b.saved = base + pb;
@@ -308,7 +312,63 @@ __global__ void p_export_kernel(const T *P, Geom g, int ncomp, double *h) {
   for (int a = 0; a < ncomp; ++a) h[t * ncomp + a] = (double)P[((long long)mu * ncomp + a) * g.V + lin];
 }
 
+__global__ void hmc_summary_kernel(const double *dH, const int *acc, int n, double *out) {
+  double a = 0.0, e = 0.0, d = 0.0;
+  for (int k = 0; k < n; ++k) {
+    a += acc[k] ? 1.0 : 0.0;
+    e += exp(-dH[k]);
+    d += dH[k];
+  }
+  out[0] = a;
+  out[1] = e;
+  out[2] = d;
+}
+
 }  // namespace
+
+namespace klft {
+
+size_t hmc_footprint(int nc, int dtype, const Geom &g, int ntraj) {
+  auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+  const size_t pb = (size_t)g.V * g.nd * ncomp_of(nc) * (dtype == 0 ? 8 : 4);
+  const size_t lb = (size_t)g.V * g.nd * nc * nc * (dtype == 0 ? 16 : 8);
+  return al(pb) + al(lb) + al(8 * sizeof(double)) + al((size_t)ntraj * sizeof(double)) +
+         al((size_t)ntraj * sizeof(int)) + (size_t)plaquette_blocks(g) * sizeof(double);
+}
+
+klft_status hmc_prepare(klft_lattice *lat, int ntraj) {
+  HmcBufs b;
+  return hmc_bufs(lat, ntraj < 1 ? 1 : ntraj, b);
+}
+
+klft_status hmc_enqueue_trajectory(klft_lattice *lat, double beta, double tau, int nsteps, int integrator, int k) {
+  HmcBufs b;
+  klft_status s = hmc_bufs(lat, k + 1, b);
+  if (s != KLFT_OK) return s;
+  CK(launch_momenta(lat, b.P));
+  if ((s = enqueue_energies(lat, b, b.slots + 0, b.slots + 1)) != KLFT_OK) return s;
+  CK(cudaMemcpyAsync(b.saved, lat->links, lat->link_bytes, cudaMemcpyDeviceToDevice, lat->stream));
+  if ((s = enqueue_integrate(lat, b, beta, tau, nsteps, integrator)) != KLFT_OK) return s;
+  if ((s = enqueue_energies(lat, b, b.slots + 2, b.slots + 3)) != KLFT_OK) return s;
+  hmc_accept_kernel<<<1, 1, 0, lat->stream>>>(b.slots, beta / (double)lat->nc, lat->seed, lat->chain,
+                                              lat->d_counters, b.dH + k, b.acc + k);
+  CK(cudaGetLastError());
+  restore_if_rejected_kernel<<<296, 256, 0, lat->stream>>>((uint4 *)lat->links, (const uint4 *)b.saved,
+                                                           (long long)(lat->link_bytes / 16), b.acc + k);
+  CK(cudaGetLastError());
+  return KLFT_OK;
+}
+
+klft_status hmc_enqueue_summary(klft_lattice *lat, int ntraj, double *d_out) {
+  HmcBufs b;
+  klft_status s = hmc_bufs(lat, ntraj < 1 ? 1 : ntraj, b);
+  if (s != KLFT_OK) return s;
+  hmc_summary_kernel<<<1, 1, 0, lat->stream>>>(b.dH, b.acc, ntraj, d_out);
+  CK(cudaGetLastError());
+  return KLFT_OK;
+}
+
+}  // namespace klft
 
 extern "C" {
 
@@ -425,20 +485,8 @@ klft_status klft_hmc_trajectories(klft_lattice *lat, double beta, double tau, in
   std::lock_guard<std::mutex> guard(lat->mtx);
   HmcBufs b;
   if ((s = hmc_bufs(lat, ntraj, b)) != KLFT_OK) return s;
-  const double bnc = beta / (double)lat->nc;
-  for (int k = 0; k < ntraj; ++k) {
-    CK(launch_momenta(lat, b.P));
-    if ((s = enqueue_energies(lat, b, b.slots + 0, b.slots + 1)) != KLFT_OK) return s;
-    CK(cudaMemcpyAsync(b.saved, lat->links, lat->link_bytes, cudaMemcpyDeviceToDevice, lat->stream));
-    if ((s = enqueue_integrate(lat, b, beta, tau, nsteps, integrator)) != KLFT_OK) return s;
-    if ((s = enqueue_energies(lat, b, b.slots + 2, b.slots + 3)) != KLFT_OK) return s;
-    hmc_accept_kernel<<<1, 1, 0, lat->stream>>>(b.slots, bnc, lat->seed, lat->chain, lat->d_counters, b.dH + k,
-                                                b.acc + k);
-    CK(cudaGetLastError());
-    restore_if_rejected_kernel<<<296, 256, 0, lat->stream>>>((uint4 *)lat->links, (const uint4 *)b.saved,
-                                                             (long long)(lat->link_bytes / 16), b.acc + k);
-    CK(cudaGetLastError());
-  }
+  for (int k = 0; k < ntraj; ++k)
+    if ((s = hmc_enqueue_trajectory(lat, beta, tau, nsteps, integrator, k)) != KLFT_OK) return s;
   if (dH_out) CK(cudaMemcpyAsync(dH_out, b.dH, (size_t)ntraj * sizeof(double), cudaMemcpyDeviceToHost, lat->stream));
   if (accepted_out)
     CK(cudaMemcpyAsync(accepted_out, b.acc, (size_t)ntraj * sizeof(int), cudaMemcpyDeviceToHost, lat->stream));
