@@ -11,6 +11,12 @@ Metric: link updates/s (a link update = one link visited by the sweep, Nd*V per
 step), for the mixed form (FP32 links, FP64 reductions; `value`) and the plain
 FP64 form (`fp64`).  Inputs are synthetic (seeded cold start).
 
+At N = 1 the same line also carries the other workloads: `batched_ptbc` (12
+PTBC SU(3) 16^4 replicas + 48 SU(2) chains per captured cycle), `hmc` (SU(2)
+24^4, 500 trajectories, mixed vs FP64), `serving` (a seeded Poisson stream of
+mixed jobs at 20 jobs/s through the job server: p50/p99 latency and aggregate
+link updates/s) and `plaquettes_per_s`.
+
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 Under torchrun (N > 1) every rank runs an independent replica (the path does
@@ -34,19 +40,25 @@ sys.path.insert(0, ROOT)
 L_DEFAULT = 32
 BETA, NHITS = 6.0, 10
 PAIRS = [(l, t) for l in range(1, 9) for t in range(1, 9)]
-METRIC = "Link updates/s (SU(3) 32^4), mixed vs FP64 form"
+METRIC = "Link updates/s (SU(3) 32^4), mixed vs FP64 form; serving p50/p99 job latency"
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--L", type=int, default=L_DEFAULT)
     ap.add_argument("--therm", type=int, default=200)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the batched-PTBC, HMC and serving legs (they run at N=1 only)")
+    ap.add_argument("--batch-cycles", type=int, default=40)
+    ap.add_argument("--hmc-traj", type=int, default=500)
+    ap.add_argument("--serve-jobs", type=int, default=100)
+    ap.add_argument("--serve-rate", type=float, default=20.0)
     return ap.parse_args()
 
 
@@ -106,10 +118,16 @@ class Clocks:
              "clocks_event_reasons.sw_power_cap")
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                          "--format=csv,noheader,nounits", "-lms", "20"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            # start the timed region only once the sampler is running; keep only
+            # the samples taken inside it
+            t_end = time.monotonic() + 3.0
+            while not self.rows and time.monotonic() < t_end and self.proc.poll() is None:
+                time.sleep(0.005)
+            self.rows.clear()
         except Exception:
             self.proc = None
         return self
@@ -231,6 +249,102 @@ def cpu_baseline_reference(L: int):
                       f"{dt:.2f} s"}
 
 
+def plaquette_ms(g, eps, reps=5):
+    """Device time of one GaugePlaquette (ms) from cycles with and without it."""
+    _, _, _, ms_sweep = g.run_cycles(BETA, 0.0, NHITS, reps, "exp", eps, False, [])
+    _, _, _, ms_plaq = g.run_cycles(BETA, 0.0, NHITS, reps, "exp", eps, True, [])
+    return max(ms_plaq - ms_sweep, 1e-6) / reps
+
+
+def bench_batched_ptbc(cycles: int, warmup: int = 3):
+    """12 PTBC replicas of SU(3) 16^4 (4^3 defect, c_r = 1 - r/11, beta = 6) plus
+    48 SU(2) chains with extents drawn from {8,12,16,20,24}^4 and beta in
+    [2.2, 2.6]: one sweep of every chain, replica swaps, every chain's
+    plaquette per cycle, one captured graph per cycle; FP32 links, FP64 sums."""
+    import klft_b200
+    rng = np.random.default_rng(2718)
+    b = klft_b200.Batch()
+    fields = []
+    links = 0
+    for r in range(12):
+        g = klft_b200.GaugeField([16] * 4, 3, "mixed", "hot", 5000 + r)
+        g.set_stream(5000, r)
+        g.set_defect(4, (0, 0, 0), 1.0)
+        b.add(g, 6.0, 0.0, NHITS, "exp", 0.25)
+        fields.append(g)
+        links += 4 * 16 ** 4
+    c_of_label = [1.0 - r / 11.0 for r in range(12)]
+    b.set_ptbc(list(range(12)), c_of_label, 6.0, 99)
+    for k in range(48):
+        L = [int(x) for x in rng.choice([8, 12, 16, 20, 24], size=4)]
+        g = klft_b200.GaugeField(L, 2, "mixed", "hot", 7000 + k)
+        g.set_stream(7000, k)
+        b.add(g, float(rng.uniform(2.2, 2.6)), 0.3, NHITS, "reference", 0.0)
+        fields.append(g)
+        links += 4 * int(np.prod(L))
+    b.run(warmup, True, True)
+    acc, plaq, lab, ms = b.run(cycles, True, True)
+    _, _, _, ms_ng = b.run(max(cycles // 4, 2), True, False)
+    swaps = b.swap_stats()
+    out = {"workload": "12 PTBC SU(3) 16^4 replicas (L_d=4, c_r=1-r/11, beta=6) + 48 SU(2) chains "
+                       "extents {8..24}^4, beta U[2.2,2.6]; per cycle 1 sweep + swaps + plaquettes, CUDA graph",
+           "chains": len(fields), "cycles": cycles, "ms_per_cycle": ms / cycles,
+           "ms_per_cycle_without_graph": ms_ng / max(cycles // 4, 2),
+           "link_updates_per_s": links * cycles / (ms * 1e-3),
+           "cycles_per_s": cycles / (ms * 1e-3),
+           "replica_acceptance": float(np.mean(acc[:, :12])), "su2_acceptance": float(np.mean(acc[:, 12:])),
+           "swaps_accepted_per_pair": [int(x) for x in swaps]}
+    b.close()
+    for g in fields:
+        g.close()
+    return out
+
+
+def bench_hmc(ntraj: int):
+    """SU(2) 24^4 HMC, beta = 2.3, tau = 1, 20 leapfrog steps, hot start: mixed vs FP64."""
+    import klft_b200
+    out = {"workload": f"SU(2) 4D 24^4 HMC beta=2.3 tau=1 20 leapfrog steps, {ntraj} trajectories from a "
+                       "hot start (seed 4242)"}
+    for prec in ("mixed", "fp64"):
+        g = klft_b200.GaugeField([24] * 4, 2, prec, "hot", 4242)
+        g.set_stream(4242, 0)
+        g.hmc(2.3, 1.0, 20, 2, "leapfrog")  # warm-up (2 trajectories, same stream continues)
+        t0 = time.perf_counter()
+        dH, acc = g.hmc(2.3, 1.0, 20, ntraj, "leapfrog")
+        dt = time.perf_counter() - t0
+        out[prec] = {"trajectories_per_s": ntraj / dt, "ms_per_trajectory": dt * 1e3 / ntraj,
+                     "acceptance": float(np.mean(acc != 0)),
+                     "acceptance_last_half": float(np.mean(acc[ntraj // 2:] != 0)),
+                     "mean_exp_mdH_last_half": float(np.mean(np.exp(np.minimum(-dH[ntraj // 2:], 700.0)))),
+                     "mean_dH_last_half": float(np.mean(dH[ntraj // 2:])),
+                     "plaquette": g.plaquette(), "unitarity": g.unitarity()}
+        g.close()
+    out["speedup_mixed_vs_fp64"] = out["mixed"]["trajectories_per_s"] / out["fp64"]["trajectories_per_s"]
+    return out
+
+
+def bench_serving(njobs: int, rate: float):
+    """A seeded Poisson stream of mixed jobs through the job server."""
+    from klft_b200.serve import Server, latency_summary, poisson_jobs, run_stream
+    jobs = poisson_jobs(njobs, rate, seed=2024)
+    with Server() as s:
+        out = run_stream(s, jobs, timeout_s=600)
+        st = s.stats()
+    res = [out["results"][i] for i in out["ids"]]
+    summ = latency_summary(res)
+    summ.update({
+        "workload": f"{njobs} jobs, Poisson arrivals at {rate} jobs/s (seed 2024): U(1)/SU(2)/SU(3), 3-4 dims, "
+                    "even extents 8..32, 50-500 Metropolis sweeps or 10-50 HMC trajectories, final plaquette and "
+                    "temporal Wilson loops; FP32 links / FP64 sums",
+        "offered_rate_jobs_per_s": rate, "failed": sum(1 for r in res if r["status"] != 0),
+        "metropolis_p99_s": float(np.percentile([r["latency"] for r in res if r["kind"] == "metropolis"], 99)),
+        "hmc_p99_s": float(np.percentile([r["latency"] for r in res if r["kind"] == "hmc"], 99)),
+        "queue_wait_p99_s": float(np.percentile([r["t_admit"] - r["t_submit"] for r in res], 99)),
+        "server": {k: st[k] for k in ("rounds", "launches", "busy_s", "completed")},
+    })
+    return summ
+
+
 def run_ours(a, dist: Dist):
     import klft_b200
     dist.set_device()
@@ -300,6 +414,17 @@ def run_ours(a, dist: Dist):
         "roofline": roofline, "e2e": e2e, "e2e_host_lattice": e2e_host,
         "clocks": clocks.summary(), "gpu_launches": launches_per_step * a.steps,
     }
+    pl_ms = plaquette_ms(g, eps)
+    line["plaquettes_per_s"] = {"value": V * 6 / (pl_ms * 1e-3), "ms": pl_ms,
+                                "note": "V*Nd(Nd-1)/2 plaquettes per GaugePlaquette, device time"}
+    if dist.world == 1 and not a.no_extras:
+        for key, fn in (("batched_ptbc", lambda: bench_batched_ptbc(a.batch_cycles)),
+                        ("hmc", lambda: bench_hmc(a.hmc_traj)),
+                        ("serving", lambda: bench_serving(a.serve_jobs, a.serve_rate))):
+            try:
+                line[key] = fn()
+            except Exception as ex:  # reported, not fatal for the headline
+                line[key] = {"error": f"{type(ex).__name__}: {ex}"}
     if dist.rank == 0 and dist.world == 1 and not a.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_baseline_reference(a.L)
