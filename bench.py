@@ -64,18 +64,23 @@ def parse():
 
 # ------------------------------------------------------------------ distributed plumbing
 class Dist:
+    """One process per GPU (torchrun env).  NCCL carries only the barrier and the
+    max-over-ranks timing; KLFT_DIST_BACKEND=gloo runs the same steps on CPU."""
+
     def __init__(self):
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.backend = os.environ.get("KLFT_DIST_BACKEND", "nccl")
         self.pg = None
         if self.world > 1:
             import datetime
 
             import torch
             import torch.distributed as dist
-            torch.cuda.set_device(self.local)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+            if self.backend == "nccl":
+                torch.cuda.set_device(self.local)
+            dist.init_process_group(self.backend, timeout=datetime.timedelta(seconds=300))
             self.pg = dist
 
     def set_device(self):
@@ -87,14 +92,18 @@ class Dist:
     def barrier(self):
         if self.pg:
             import torch
-            self.pg.barrier(device_ids=[self.local])
-            torch.cuda.synchronize()
+            if self.backend == "nccl":
+                self.pg.barrier(device_ids=[self.local])
+                torch.cuda.synchronize()
+            else:
+                self.pg.barrier()
 
     def max(self, x: float) -> float:
         if not self.pg:
             return x
         import torch
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{self.local}")
+        dev = f"cuda:{self.local}" if self.backend == "nccl" else "cpu"
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
         self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
         return float(t.item())
 

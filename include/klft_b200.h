@@ -186,6 +186,20 @@ klft_status klft_tuner_write_cache(const char *path);
 klft_status klft_tuner_lookup(const char *key, int *values, int *rank);
 klft_status klft_tuner_clear(void);
 
+/* ---------------------------------------------------------------- checkpoints
+ * No counterpart in the reference (it has no configuration I/O; measurements
+ * live in host vectors until a run ends, GaugeObservable.hpp:40-44).  A
+ * checkpoint holds the links (host interchange layout, complex128; the mixed
+ * form's FP32 values convert exactly), the Philox stream (seed, chain), the
+ * sweep/trajectory/cycle counters and the PTBC defect, with FNV-1a checksums of
+ * header and payload.  Random numbers depend only on those, so a lattice read
+ * back continues bit for bit where the written one stopped.  Writes go to
+ * "<path>.tmp" and are renamed into place. */
+klft_status klft_checkpoint_write(klft_lattice *lat, const char *path);
+/* KLFT_EINVAL for a missing, foreign, truncated or corrupted file (checked
+ * before any device work). */
+klft_status klft_checkpoint_read(const char *path, klft_lattice **out);
+
 /* ---------------------------------------------------------------- serving
  * No counterpart in the reference (its only drivers are the metropolis and hmc
  * binaries, Metropolis.hpp:113-223 and HMC.hpp:20-117, one run per process).

@@ -16,6 +16,7 @@ libklft_b200.so (include/klft_b200.h).  Names follow klft:
 from __future__ import annotations
 
 import ctypes as C
+import os
 from dataclasses import dataclass, field
 from typing import List, Sequence, Tuple
 
@@ -58,6 +59,27 @@ class GaugeField:
         h = C.c_void_p()
         check(lib().klft_lattice_create(self.nc, self.nd, Lc, PRECISION[precision], START[start], seed, C.byref(h)))
         self._h = h
+
+    @classmethod
+    def load(cls, path: str) -> "GaugeField":
+        """A lattice restored from a checkpoint (klft_checkpoint_read)."""
+        h = C.c_void_p()
+        check(lib().klft_checkpoint_read(os.fsencode(path), C.byref(h)))
+        g = cls.__new__(cls)
+        g._h = h
+        nc, nd, prec = C.c_int(), C.c_int(), C.c_int()
+        Lc = (C.c_int * 4)()
+        V = C.c_longlong()
+        check(lib().klft_lattice_info(h, C.byref(nc), C.byref(nd), Lc, C.byref(prec), C.byref(V)))
+        g.nc, g.nd = nc.value, nd.value
+        g.L = [Lc[d] for d in range(g.nd)]
+        g.precision = {v: k for k, v in PRECISION.items()}[prec.value]
+        g.V = V.value
+        return g
+
+    def save(self, path: str) -> None:
+        """Write a checkpoint: links, Philox stream, counters, defect (klft_checkpoint_write)."""
+        check(lib().klft_checkpoint_write(self._h, os.fsencode(path)))
 
     # -- lifetime
     def close(self):
