@@ -38,9 +38,11 @@ typedef enum {
 
 typedef enum { KLFT_PRECISION_FP64 = 0, KLFT_PRECISION_MIXED = 1 } klft_precision;
 typedef enum { KLFT_START_COLD = 0, KLFT_START_HOT = 1 } klft_start;
-/* SU(3) proposal: the reference Gram-Schmidt generator (SUN.hpp:192-251) or
- * X = exp(i eps H), H hermitian traceless Gaussian.  U(1)/SU(2) always use the
- * reference generators (SUN.hpp:163-189). */
+/* SU(3) proposal: the reference Gram-Schmidt generator (SUN.hpp:192-251),
+ * U' = U r as in Metropolis.hpp:91, or U' = X U with X = exp(i eps H), H
+ * hermitian traceless Gaussian; accepted X U products are reunitarised once
+ * after the link's hits.  U(1)/SU(2) always use the reference generators
+ * (SUN.hpp:163-189). */
 typedef enum { KLFT_PROPOSAL_REFERENCE = 0, KLFT_PROPOSAL_EXP = 1 } klft_proposal;
 
 typedef struct klft_lattice klft_lattice;

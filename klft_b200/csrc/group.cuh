@@ -41,8 +41,12 @@ template <typename T> KLFT_D Mat<3, T> herm_square(const Mat<3, T> &Q) {
 struct FastMath {
   static KLFT_D float fsin(float x) { return __sinf(x); }
   static KLFT_D float fcos(float x) { return __cosf(x); }
+  static KLFT_D float frsqrt(float x) { return rsqrtf(x); }
+  static KLFT_D float frcp(float x) { return __fdividef(1.0f, x); }
   static KLFT_D double fsin(double x) { return sin(x); }
   static KLFT_D double fcos(double x) { return cos(x); }
+  static KLFT_D double frsqrt(double x) { return 1.0 / sqrt(x); }
+  static KLFT_D double frcp(double x) { return 1.0 / x; }
 };
 
 template <typename T> KLFT_D Mat<3, T> expi_su3(const Mat<3, T> &Q) {
@@ -63,18 +67,21 @@ template <typename T> KLFT_D Mat<3, T> expi_su3(const Mat<3, T> &Q) {
   } else {
     const bool neg = c0 < T(0);
     const T ac0 = neg ? -c0 : c0;
-    const T c0max = T(2) * (c1 / T(3)) * sqrt(c1 / T(3));
-    T ratio = ac0 / c0max;
+    // with r = (c1/3)^(-1/2): sqrt(c1/3) = (c1/3) r, c0max = 2 (c1/3)^(3/2)
+    const T c13 = c1 * T(1.0 / 3.0);
+    const T r = FastMath::frsqrt(c13);
+    const T s13 = c13 * r;
+    T ratio = T(0.5) * ac0 * (r * r * r);
     ratio = ratio > T(1) ? T(1) : ratio;
     const T theta = acos(ratio);
-    const T u = sqrt(c1 / T(3)) * FastMath::fcos(theta / T(3));
-    const T w = sqrt(c1) * FastMath::fsin(theta / T(3));
+    const T u = s13 * FastMath::fcos(theta * T(1.0 / 3.0));
+    const T w = T(1.7320508075688772) * s13 * FastMath::fsin(theta * T(1.0 / 3.0));
     const T u2 = u * u, w2 = w * w;
     T xi0;
     if (fabs(w) < T(0.05)) {
-      xi0 = T(1) - w2 / T(6) * (T(1) - w2 / T(20) * (T(1) - w2 / T(42)));
+      xi0 = T(1) - w2 * T(1.0 / 6.0) * (T(1) - w2 * T(1.0 / 20.0) * (T(1) - w2 * T(1.0 / 42.0)));
     } else {
-      xi0 = FastMath::fsin(w) / w;
+      xi0 = FastMath::fsin(w) * FastMath::frcp(w);
     }
     const T cw = FastMath::fcos(w);
     const T s2u = FastMath::fsin(T(2) * u), c2u = FastMath::fcos(T(2) * u);
@@ -84,10 +91,11 @@ template <typename T> KLFT_D Mat<3, T> expi_su3(const Mat<3, T> &Q) {
     const cx<T> h0 = e2iu * (u2 - w2) + emiu * mk<T>(T(8) * u2 * cw, T(2) * u * (T(3) * u2 + w2) * xi0);
     const cx<T> h1 = e2iu * (T(2) * u) - emiu * mk<T>(T(2) * u * cw, -(T(3) * u2 - w2) * xi0);
     const cx<T> h2 = e2iu - emiu * mk<T>(cw, T(3) * u * xi0);
-    const T den = T(9) * u2 - w2;
-    f0 = cdiv(h0, den);
-    f1 = cdiv(h1, den);
-    f2 = cdiv(h2, den);
+    // 9u^2 - w^2 = c1 (3 cos^2(theta/3) - sin^2(theta/3)) >= 2 c1 for theta in [0, pi/2]
+    const T iden = FastMath::frcp(T(9) * u2 - w2);
+    f0 = mk<T>(h0.re * iden, h0.im * iden);
+    f1 = mk<T>(h1.re * iden, h1.im * iden);
+    f2 = mk<T>(h2.re * iden, h2.im * iden);
     if (neg) {  // f_j(-c0) = (-1)^j conj(f_j(c0))
       f0 = conj(f0);
       f1 = mk<T>(-f1.re, f1.im);

@@ -27,21 +27,24 @@
 namespace klft {
 
 // Fixed-position stream of the exp(i eps H) proposal: hit h of a site
-// (h = mu*nHits + hit) uses Philox blocks 3h, 3h+1 (eight 32-bit uniforms
-// u = (w + 1/2) 2^-32 for four Box-Muller pairs) and 3h+2 (53-bit accept
-// uniform) of the (sweep, site) counter.
+// (h = mu*nHits + hit) uses Philox blocks 2h, 2h+1 of sub-stream 0 (eight
+// 32-bit uniforms u = (w + 1/2) 2^-32 for four Box-Muller pairs) and word h mod 4
+// of block h / 4 of sub-stream 1 for its accept uniform (w + 1/2) 2^-32, so one
+// block serves the accept decisions of four hits.
 struct ExpHitStream {
   uint32_t k0, k1, site, step;
-  KLFT_D void block(uint32_t b, uint32_t w[4]) const {
-    w[0] = b; w[1] = site; w[2] = step; w[3] = KIND_METROPOLIS << 24;
+  KLFT_D void block(uint32_t b, uint32_t w[4], uint32_t sub = 0) const {
+    w[0] = b; w[1] = site; w[2] = step; w[3] = (KIND_METROPOLIS << 24) | sub;
     philox4x32_10(w, k0, k1);
   }
-  KLFT_D double accept_uniform(uint32_t h) const {
-    uint32_t w[4];
-    block(3 * h + 2, w);
-    return (double)((((uint64_t)w[0] << 32) | w[1]) >> 11) * 0x1.0p-53;
-  }
+  KLFT_D void accept_block(uint32_t h, uint32_t w[4]) const { block(h >> 2, w, 1); }
 };
+
+KLFT_D double accept_word(const uint32_t w[4], uint32_t h) {
+  const uint32_t j = h & 3;
+  const uint32_t x = j == 0 ? w[0] : (j == 1 ? w[1] : (j == 2 ? w[2] : w[3]));
+  return ((double)x + 0.5) * 0x1.0p-32;
+}
 
 KLFT_D void box_muller(uint32_t wa, uint32_t wb, double &g0, double &g1) {
   const double ua = ((double)wa + 0.5) * 0x1.0p-32, ub = ((double)wb + 0.5) * 0x1.0p-32;
@@ -51,11 +54,13 @@ KLFT_D void box_muller(uint32_t wa, uint32_t wb, double &g0, double &g1) {
   g0 = r * c;
   g1 = r * s;
 }
-// Mixed form: SFU log and sincos.  cos/sin(2 pi u) = -cos/sin(2 pi (u - 1/2)) keeps
-// the SFU argument in [-pi, pi].
+// Mixed form: SFU log, rsqrt and sincos.  cos/sin(2 pi u) = -cos/sin(2 pi (u - 1/2))
+// keeps the SFU argument in [-pi, pi]; ua rounds to 1 for the largest words,
+// where the radius is 0.
 KLFT_D void box_muller(uint32_t wa, uint32_t wb, float &g0, float &g1) {
   const float ua = fmaf((float)wa, 0x1.0p-32f, 0x1.0p-33f), ub = fmaf((float)wb, 0x1.0p-32f, 0x1.0p-33f);
-  const float r = sqrtf(-2.0f * __logf(ua));
+  const float q = -2.0f * __logf(ua);
+  const float r = q > 0.0f ? q * rsqrtf(q) : 0.0f;
   float s, c;
   __sincosf(6.28318530717958648f * (ub - 0.5f), &s, &c);
   g0 = -r * c;
@@ -65,8 +70,8 @@ KLFT_D void box_muller(uint32_t wa, uint32_t wb, float &g0, float &g1) {
 template <typename T>
 KLFT_D Mat<3, T> exp_proposal(const ExpHitStream &hs, uint32_t h, T half_eps) {
   uint32_t w[8];
-  hs.block(3 * h, w);
-  hs.block(3 * h + 1, w + 4);
+  hs.block(2 * h, w);
+  hs.block(2 * h + 1, w + 4);
   T g[8];
 #pragma unroll
   for (int k = 0; k < 4; ++k) box_muller(w[2 * k], w[2 * k + 1], g[2 * k], g[2 * k + 1]);
@@ -145,13 +150,15 @@ KLFT_D int site_update_ref(const Links<NC, T> &U, const Geom &g, const Site &x, 
   return nacc;
 }
 
-// SU(3) exp(i eps H) proposals at fixed stream positions.  Staple and link wait
-// in shared memory (read only on acceptance: M = S U), one structure-of-arrays
-// slot per thread, leaving registers to the proposal.
+// SU(3) exp(i eps H) proposals U' = X U at fixed stream positions.
+// Re Tr(X U S) = Re Tr(X M) with M = U S carried in registers; an accepted
+// proposal updates U <- X U and M <- X M (no reprojection between hits: X is
+// unitary to round-off) and the link is reunitarised once after its hits.  The link waits in shared memory, one
+// structure-of-arrays slot per thread, leaving registers to the proposal; the
+// staple is not needed after M is formed.
 template <int ND, typename T, bool DF>
 KLFT_D int site_update_exp(const Links<3, T> &U, const Geom &g, const Site &x, const MetroArgs &a, uint32_t sweep,
                            const Defect &df) {
-  __shared__ cx<T> s_S[9][128];
   __shared__ cx<T> s_U[9][128];
   const int tid = threadIdx.x;
   int nacc = 0;
@@ -167,34 +174,29 @@ KLFT_D int site_update_exp(const Links<3, T> &U, const Geom &g, const Site &x, c
       const Mat<3, T> Uo = U.load(lx, mu);
       const Mat<3, T> S = staple<3, ND, T, DF>(U, g, x, mu, df);
 #pragma unroll
-      for (int k = 0; k < 9; ++k) {
-        s_S[k][tid] = S.e[k / 3][k % 3];
-        s_U[k][tid] = Uo.e[k / 3][k % 3];
-      }
-      M = mul(S, Uo);
+      for (int k = 0; k < 9; ++k) s_U[k][tid] = Uo.e[k / 3][k % 3];
+      M = mul(Uo, S);
     }
-    Mat<3, T> rr;
     const bool dlink = DF && df.active && in_defect(g, df, x, mu);
     T trO = retr_diag(M);
     bool changed = false;
+    uint32_t aw[4];
 #pragma unroll 1
     for (int hit = 0; hit < a.nhits; ++hit) {
-      rr = exp_proposal<T>(hs, h0 + hit, half_eps);
+      const uint32_t h = h0 + (uint32_t)hit;
+      if (hit == 0 || (h & 3u) == 0u) hs.accept_block(h, aw);
+      const Mat<3, T> rr = exp_proposal<T>(hs, h, half_eps);
       T dS = -bnc * (retr_mul(rr, M) - trO);
       if (dlink) dS *= (T)defect_c(df);
-      bool accept = dS < T(0);
-      if (!accept) accept = hs.accept_uniform(h0 + hit) < (double)exp(-dS);
+      const bool accept = dS < T(0) || accept_word(aw, h) < (double)exp(-dS);
       if (accept) {
-        Mat<3, T> Uo, S;
+        Mat<3, T> Uo;
 #pragma unroll
         for (int k = 0; k < 9; ++k) Uo.e[k / 3][k % 3] = s_U[k][tid];
-        Uo = restore(mul(Uo, rr));
+        Uo = mul(rr, Uo);
 #pragma unroll
-        for (int k = 0; k < 9; ++k) {
-          s_U[k][tid] = Uo.e[k / 3][k % 3];
-          S.e[k / 3][k % 3] = s_S[k][tid];
-        }
-        M = mul(S, Uo);
+        for (int k = 0; k < 9; ++k) s_U[k][tid] = Uo.e[k / 3][k % 3];
+        M = mul(rr, M);
         trO = retr_diag(M);
         ++nacc;
         changed = true;
@@ -204,7 +206,7 @@ KLFT_D int site_update_exp(const Links<3, T> &U, const Geom &g, const Site &x, c
       Mat<3, T> Uo;
 #pragma unroll
       for (int k = 0; k < 9; ++k) Uo.e[k / 3][k % 3] = s_U[k][tid];
-      U.store(lx, mu, Uo);
+      U.store(lx, mu, restore(Uo));
     }
   }
   return nacc;

@@ -237,9 +237,10 @@ static inline void randsun(Mat<2> &r, Stream &g, double delta, int, double) {
 // Project SU(3) proposal X = exp(i eps H), H = sum_a h_a lambda_a / 2, h_a ~ N(0,1).
 // It has no counterpart in the reference, so its random numbers sit at fixed
 // positions of the (sweep, site) stream: hit h of the site (h = mu*nHits + hit)
-// takes Philox blocks 3h and 3h+1 for eight 32-bit uniforms u = (w + 1/2) 2^-32
-// (Box-Muller pairs (u0,u1), (u2,u3), (u4,u5), (u6,u7)) and block 3h+2 for the
-// 53-bit accept uniform.  A proposal therefore does not depend on earlier accept
+// takes Philox blocks 2h and 2h+1 (sub-stream 0) for eight 32-bit uniforms
+// u = (w + 1/2) 2^-32 (Box-Muller pairs (u0,u1), (u2,u3), (u4,u5), (u6,u7)), and
+// word h mod 4 of block h / 4 of sub-stream 1 for its accept uniform
+// (w + 1/2) 2^-32.  A proposal therefore does not depend on earlier accept
 // decisions.
 struct ExpHit {
   uint32_t key[2], site, step;
@@ -247,14 +248,14 @@ struct ExpHit {
     key[0] = (uint32_t)seed;
     key[1] = (uint32_t)(seed >> 32) ^ (uint32_t)chain;
   }
-  void block(uint32_t b, uint32_t out[4]) const {
-    uint32_t ctr[4] = {b, site, step, KIND_METROPOLIS << 24};
+  void block(uint32_t b, uint32_t out[4], uint32_t sub = 0) const {
+    uint32_t ctr[4] = {b, site, step, (KIND_METROPOLIS << 24) | sub};
     philox(ctr, key, out);
   }
   void gauss8(uint32_t h, double g[8]) const {
     uint32_t w[8];
-    block(3 * h, w);
-    block(3 * h + 1, w + 4);
+    block(2 * h, w);
+    block(2 * h + 1, w + 4);
     for (int k = 0; k < 4; ++k) {
       const double ua = ((double)w[2 * k] + 0.5) * 0x1.0p-32, ub = ((double)w[2 * k + 1] + 0.5) * 0x1.0p-32;
       const double r = std::sqrt(-2.0 * std::log(ua));
@@ -264,8 +265,8 @@ struct ExpHit {
   }
   double accept_uniform(uint32_t h) const {
     uint32_t w[4];
-    block(3 * h + 2, w);
-    return (double)((((uint64_t)w[0] << 32) | w[1]) >> 11) * 0x1.0p-53;
+    block(h >> 2, w, 1);
+    return ((double)w[h & 3] + 0.5) * 0x1.0p-32;
   }
 };
 
@@ -476,6 +477,10 @@ static double metropolis_sweep(const Field<NC> &F, double beta, double delta, in
       for (int mu = 0; mu < nd; ++mu) {
         const Mat<NC> S = staple(F, s, mu);
         const double c = link_factor(g, F.df, s, mu);
+        // exp(i eps H) proposals: accepted products U r are kept unprojected
+        // while the link's hits run and reunitarised once at the end
+        Mat<NC> Ucur = F.raw(s, mu);
+        bool changed = false;
         for (int hit = 0; hit < nHits; ++hit) {
           const uint32_t h = (uint32_t)(mu * nHits + hit);
           Mat<NC> r;
@@ -485,17 +490,24 @@ static double metropolis_sweep(const Field<NC> &F, double beta, double delta, in
           } else {
             randsun(r, rng, delta, proposal, eps);
           }
-          const Mat<NC> Uold = F.raw(s, mu);
-          const Mat<NC> Unew = mul(Uold, r);
+          // reference proposals U r (Metropolis.hpp:91); exp(i eps H) proposals X U
+          const Mat<NC> Uold = expprop ? Ucur : F.raw(s, mu);
+          const Mat<NC> Unew = expprop ? mul(r, Uold) : mul(Uold, r);
           double dS = -(beta / (double)NC) * (trace(mul(Unew, S)).real() - trace(mul(Uold, S)).real());
           if (c != 1.0) dS *= c;
           bool accept = dS < 0.0;
           if (!accept) accept = ((expprop ? eh.accept_uniform(h) : rng.drand(0.0, 1.0)) < std::exp(-dS));
           if (accept) {
-            F.put(s, mu, restore(Unew));
+            if (expprop) {
+              Ucur = Unew;
+              changed = true;
+            } else {
+              F.put(s, mu, restore(Unew));
+            }
             ++nacc;
           }
         }
+        if (changed) F.put(s, mu, restore(Ucur));
       }
     }
   }
