@@ -520,21 +520,20 @@ klft_status make_wilson_plan(klft_lattice *lat, const int *pairs, int npairs, in
     if (pairs[2 * k] == 0 || pairs[2 * k + 1] == 0) degenerate = true;
   }
   const size_t smem = wilson_gf_smem(lat->nc, lat->dtype(), lat->g, nu, plan.tmax, npairs);
-  plan.gf = !degenerate && npairs > 0 && smem <= 200 * 1024;
-  std::vector<int> h;
-  h.insert(h.end(), pairs, pairs + 2 * npairs);
+  plan.gf = !degenerate && npairs > 0 && npairs <= WL_MAXP && plan.lmax <= WL_MAXP && plan.tmax <= 32767 &&
+            smem <= 200 * 1024;
+  std::vector<int> h(pairs, pairs + 2 * npairs);
   if (plan.gf) {
-    std::vector<int> off(plan.lmax + 2, 0), tl, pl;
+    plan.off.assign(plan.lmax + 2, 0);
     for (int L = 1; L <= plan.lmax; ++L) {
-      off[L] = (int)tl.size();
+      plan.off[L] = (int)plan.T.size();
       for (int k = 0; k < npairs; ++k)
-        if (pairs[2 * k] == L) { tl.push_back(pairs[2 * k + 1]); pl.push_back(k); }
+        if (pairs[2 * k] == L) {
+          plan.T.push_back(pairs[2 * k + 1]);
+          plan.p.push_back(k);
+        }
     }
-    off[plan.lmax + 1] = (int)tl.size();
-    off[0] = 0;
-    plan.off_at = (int)h.size(); h.insert(h.end(), off.begin(), off.end());
-    plan.t_at = (int)h.size(); h.insert(h.end(), tl.begin(), tl.end());
-    plan.p_at = (int)h.size(); h.insert(h.end(), pl.begin(), pl.end());
+    plan.off[plan.lmax + 1] = (int)plan.T.size();
     CK(lat->s_gf.ensure(wilson_gf_scratch(lat->nc, lat->dtype(), lat->g, nu, plan.tmax)));
   }
   CK(lat->s_tab.ensure(h.size() * sizeof(int) + 16));
@@ -550,10 +549,10 @@ klft_status enqueue_wilson_plane(klft_lattice *lat, const WilsonPlan &plan, int 
                                  double *d_out) {
   const int *tab = (const int *)lat->s_tab.ptr;
   if (plan.gf) {
-    const int *dt[3] = {tab + plan.off_at, tab + plan.t_at, tab + plan.p_at};
-    CK(launch_wilson_gf(lat->nc, lat->dtype(), lat->links, lat->g, mu, nu, dt, nullptr, plan.lmax, plan.tmax,
-                        plan.npairs, omega_ready, lat->s_gf.ptr, (double *)lat->s_part.ptr, wilson_gf_blocks(lat->g),
-                        d_out, lat->stream));
+    const int *ht[3] = {plan.off.data(), plan.T.data(), plan.p.data()};
+    CK(launch_wilson_gf(lat->nc, lat->dtype(), lat->links, lat->g, mu, nu, ht, plan.lmax, plan.tmax, plan.npairs,
+                        omega_ready, lat->s_gf.ptr, (double *)lat->s_part.ptr, wilson_gf_blocks(lat->g), d_out,
+                        lat->stream));
   } else {
     const int nblk = plaquette_blocks(lat->g);
     CK(launch_wilson_direct(lat->nc, lat->dtype(), lat->links, lat->g, mu, nu, tab, plan.npairs,

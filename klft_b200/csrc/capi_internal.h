@@ -76,11 +76,13 @@ klft_status hmc_enqueue_summary(klft_lattice *lat, int ntraj, double *d_out);
 // device bytes of the HMC buffers for ntraj trajectories
 size_t hmc_footprint(int nc, int dtype, const Geom &g, int ntraj);
 
-// Device tables of a Wilson-loop pair list (offsets are int indices into s_tab).
+// A Wilson-loop pair list: the pairs on the device (direct form, in s_tab) and
+// the per-length tables the gauge-fixed kernel takes in its parameters.
 struct WilsonPlan {
   int npairs = 0, lmax = 0, tmax = 0;
   bool gf = false;
-  int off_at = 0, t_at = 0, p_at = 0;
+  // gauge-fixed form: loops of length L are entries off[L] .. off[L+1]-1 of (T, pair)
+  std::vector<int> off, T, p;
 };
 klft_status make_wilson_plan(klft_lattice *lat, const int *pairs, int npairs, int nu, WilsonPlan &plan);
 klft_status enqueue_wilson_plane(klft_lattice *lat, const WilsonPlan &plan, int mu, int nu, bool omega_ready,

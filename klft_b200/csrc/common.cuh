@@ -257,12 +257,31 @@ struct Geom {
   int H[4];      // half extents
   int hs[4];     // hidx strides
   long long V, Vh;
+  // select-based access for directions known only at run time, so that a kernel
+  // parameter Geom is read from the constant bank instead of a local copy
+  KLFT_HD int Ld(int d) const { return d == 0 ? L[0] : (d == 1 ? L[1] : (d == 2 ? L[2] : L[3])); }
+  KLFT_HD int Hd(int d) const { return d == 0 ? H[0] : (d == 1 ? H[1] : (d == 2 ? H[2] : H[3])); }
 };
 
-// A site held as parity bits + half coordinates.
+// A site as parity bits b_d = x_d & 1 and half-lattice coordinates h_d = x_d / 2.
+// Scalar members with select-based access: a direction known only at run time
+// (the rolled staple loops) costs a few selects instead of a local-memory array.
 struct Site {
-  int b[4];
-  int h[4];
+  int b0 = 0, b1 = 0, b2 = 0, b3 = 0, h0 = 0, h1 = 0, h2 = 0, h3 = 0;
+  KLFT_HD int b(int d) const { return d == 0 ? b0 : (d == 1 ? b1 : (d == 2 ? b2 : b3)); }
+  KLFT_HD int h(int d) const { return d == 0 ? h0 : (d == 1 ? h1 : (d == 2 ? h2 : h3)); }
+  KLFT_HD void set_b(int d, int v) {
+    b0 = d == 0 ? v : b0;
+    b1 = d == 1 ? v : b1;
+    b2 = d == 2 ? v : b2;
+    b3 = d == 3 ? v : b3;
+  }
+  KLFT_HD void set_h(int d, int v) {
+    h0 = d == 0 ? v : h0;
+    h1 = d == 1 ? v : h1;
+    h2 = d == 2 ? v : h2;
+    h3 = d == 3 ? v : h3;
+  }
 };
 
 KLFT_HD long long site_lin(const Geom &g, const Site &s) {
@@ -270,8 +289,8 @@ KLFT_HD long long site_lin(const Geom &g, const Site &s) {
   long long hidx = 0;
 #pragma unroll
   for (int d = 0; d < 4; ++d) {
-    sub |= s.b[d] << d;
-    hidx += (long long)s.h[d] * g.hs[d];
+    sub |= s.b(d) << d;
+    hidx += (long long)s.h(d) * g.hs[d];
   }
   return (long long)sub * g.Vh + hidx;
 }
@@ -279,35 +298,35 @@ KLFT_HD long long site_lin(const Geom &g, const Site &s) {
 KLFT_HD uint32_t site_lex(const Geom &g, const Site &s) {
   uint32_t lex = 0;
 #pragma unroll
-  for (int d = 3; d >= 0; --d) lex = lex * (uint32_t)g.L[d] + (uint32_t)(2 * s.h[d] + s.b[d]);
+  for (int d = 3; d >= 0; --d) lex = lex * (uint32_t)g.L[d] + (uint32_t)(2 * s.h(d) + s.b(d));
   return lex;
 }
 // x + e_d (periodic)
 KLFT_HD Site site_up(const Geom &g, Site s, int d) {
-  if (s.b[d] == 0) {
-    s.b[d] = 1;
+  if (s.b(d) == 0) {
+    s.set_b(d, 1);
   } else {
-    s.b[d] = 0;
-    s.h[d] = (s.h[d] + 1 == g.H[d]) ? 0 : s.h[d] + 1;
+    s.set_b(d, 0);
+    s.set_h(d, (s.h(d) + 1 == g.Hd(d)) ? 0 : s.h(d) + 1);
   }
   return s;
 }
 // x - e_d (periodic)
 KLFT_HD Site site_dn(const Geom &g, Site s, int d) {
-  if (s.b[d] == 1) {
-    s.b[d] = 0;
+  if (s.b(d) == 1) {
+    s.set_b(d, 0);
   } else {
-    s.b[d] = 1;
-    s.h[d] = (s.h[d] == 0) ? g.H[d] - 1 : s.h[d] - 1;
+    s.set_b(d, 1);
+    s.set_h(d, (s.h(d) == 0) ? g.Hd(d) - 1 : s.h(d) - 1);
   }
   return s;
 }
 // x + k e_d, any k >= 0 (periodic)
 KLFT_HD Site site_shift(const Geom &g, Site s, int d, int k) {
-  int x = 2 * s.h[d] + s.b[d];
-  x = (x + k) % g.L[d];
-  s.b[d] = x & 1;
-  s.h[d] = x >> 1;
+  int x = 2 * s.h(d) + s.b(d);
+  x = (x + k) % g.Ld(d);
+  s.set_b(d, x & 1);
+  s.set_h(d, x >> 1);
   return s;
 }
 KLFT_HD Site site_from_lin(const Geom &g, long long lin) {
@@ -316,8 +335,8 @@ KLFT_HD Site site_from_lin(const Geom &g, long long lin) {
   long long hidx = lin - (long long)sub * g.Vh;
 #pragma unroll
   for (int d = 0; d < 4; ++d) {
-    s.b[d] = (sub >> d) & 1;
-    s.h[d] = (int)(hidx % g.H[d]);
+    s.set_b(d, (sub >> d) & 1);
+    s.set_h(d, (int)(hidx % g.H[d]));
     hidx /= g.H[d];
   }
   return s;
@@ -328,8 +347,8 @@ KLFT_HD Site site_from_lex(const Geom &g, long long lex) {
   for (int d = 0; d < 4; ++d) {
     const int x = (int)(lex % g.L[d]);
     lex /= g.L[d];
-    s.b[d] = x & 1;
-    s.h[d] = x >> 1;
+    s.set_b(d, x & 1);
+    s.set_h(d, x >> 1);
   }
   return s;
 }
@@ -374,9 +393,9 @@ KLFT_HD double defect_c(const Defect &df) {
 }
 KLFT_HD bool in_defect(const Geom &g, const Defect &df, const Site &s, int mu) {
   if (!df.active || mu != 0) return false;
-  if (2 * s.h[0] + s.b[0] != 0) return false;
+  if (2 * s.h(0) + s.b(0) != 0) return false;
   for (int d = 1; d < g.nd; ++d) {
-    int rel = (2 * s.h[d] + s.b[d]) - df.pos[d - 1];
+    int rel = (2 * s.h(d) + s.b(d)) - df.pos[d - 1];
     rel %= g.L[d];
     if (rel < 0) rel += g.L[d];
     if (rel >= df.len) return false;

@@ -42,10 +42,12 @@ cudaError_t launch_wilson_direct(int nc, int dtype, const void *links, const Geo
 size_t wilson_gf_scratch(int nc, int dtype, const Geom &g, int nu, int tmax);
 size_t wilson_gf_smem(int nc, int dtype, const Geom &g, int nu, int tmax, int npairs);
 int wilson_gf_blocks(const Geom &g);
+// h_tab = {off[lmax+2], T[npairs], p[npairs]} on the host (passed in the kernel
+// parameters); npairs, lmax <= WL_MAXP
+constexpr int WL_MAXP = 128;
 cudaError_t launch_wilson_gf(int nc, int dtype, const void *links, const Geom &g, int mu, int nu,
-                             const int *const *d_tab, const int *h_off, int lmax, int tmax, int npairs,
-                             bool omega_ready, void *scratch, double *d_part, int nblk, double *d_out,
-                             cudaStream_t st);
+                             const int *const *h_tab, int lmax, int tmax, int npairs, bool omega_ready,
+                             void *scratch, double *d_part, int nblk, double *d_out, cudaStream_t st);
 
 int plaquette_blocks(const Geom &g);
 // ordered final reduction of nblk partials for each of n outputs

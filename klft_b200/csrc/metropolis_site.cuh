@@ -104,9 +104,9 @@ KLFT_D Site pass_site(const Geom &g, long long t, int val, int nd) {
   Site x;
 #pragma unroll
   for (int d = 0; d < 4; ++d) {
-    x.h[d] = (int)(t % g.H[d]);
+    x.set_h(d, (int)(t % g.H[d]));
     t /= g.H[d];
-    x.b[d] = d < nd ? (val >> (nd - 1 - d)) & 1 : 0;
+    x.set_b(d, d < nd ? (val >> (nd - 1 - d)) & 1 : 0);
   }
   return x;
 }

@@ -44,8 +44,8 @@ KLFT_D bool window_site(const Geom &g, long long t, Site &x, long long &lin) {
   long long r = hidx;
 #pragma unroll
   for (int d = 0; d < 4; ++d) {
-    x.b[d] = (sub >> d) & 1;
-    x.h[d] = (int)(r % g.H[d]);
+    x.set_b(d, (sub >> d) & 1);
+    x.set_h(d, (int)(r % g.H[d]));
     r /= g.H[d];
   }
   lin = (long long)sub * g.Vh + hidx;

@@ -32,15 +32,15 @@ __global__ void defect_sums_kernel(Links<NC, T> U, Geom g, Defect df, double bnc
   if (t < nsp) {
     // spatial coordinates x1.. of this thread, x0 = 0
     Site x;
-    x.b[0] = 0;
-    x.h[0] = 0;
+    x.set_b(0, 0);
+    x.set_h(0, 0);
     long long r = t;
 #pragma unroll
     for (int d = 1; d < 4; ++d) {
       const int xd = (int)(r % g.L[d]);
       r /= g.L[d];
-      x.b[d] = xd & 1;
-      x.h[d] = xd >> 1;
+      x.set_b(d, xd & 1);
+      x.set_h(d, xd >> 1);
     }
     const bool here = in_defect(g, df, x, 0);
     const Mat<NC, T> u0 = U.load(site_lin(g, x), 0);

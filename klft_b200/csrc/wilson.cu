@@ -24,6 +24,8 @@
 // Omega and U' are stored "column major": entry (column c, row b) at c*rows + b,
 // one plane per complex colour entry, so a warp covering consecutive rows of
 // one column reads contiguous memory.
+#include <cstring>
+
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -35,6 +37,7 @@ struct ColGeom {
   int cs[4];      // column stride of each dimension (0 for nu)
   long long ncols;
   int rows;       // stored rows of U' (L_nu + extension)
+  int Lmu, Lnu, csmu;  // L[mu], L[nu], cs[mu] (kernel parameters indexed by a run-time mu would be copied)
 };
 
 KLFT_HD ColGeom make_colgeom(const Geom &g, int mu, int nu, int rows) {
@@ -54,6 +57,9 @@ KLFT_HD ColGeom make_colgeom(const Geom &g, int mu, int nu, int rows) {
   }
   c.ncols = s;
   c.rows = rows;
+  c.Lmu = g.L[mu];
+  c.Lnu = g.L[nu];
+  c.csmu = c.cs[mu];
   return c;
 }
 
@@ -71,18 +77,18 @@ KLFT_D Site col_site(const ColGeom &c, long long col, int row) {
     } else {
       x = 0;
     }
-    s.b[d] = x & 1;
-    s.h[d] = x >> 1;
+    s.set_b(d, x & 1);
+    s.set_h(d, x >> 1);
   }
   return s;
 }
 
 // column index of xbar + k mu
 KLFT_D long long col_shift(const ColGeom &c, long long col, int k) {
-  const int Lm = c.L[c.mu];
-  const int xm = (int)((col / c.cs[c.mu]) % Lm);
+  const int Lm = c.Lmu;
+  const int xm = (int)((col / c.csmu) % Lm);
   const int xn = (xm + k) % Lm;
-  return col + (long long)(xn - xm) * c.cs[c.mu];
+  return col + (long long)(xn - xm) * c.csmu;
 }
 
 template <int N, typename T> struct CField {
@@ -129,7 +135,7 @@ template <int N, typename T>
 __global__ void omega_kernel(Links<N, T> U, Geom g, ColGeom c, CField<N, T> om, CField<N, T> pol) {
   const long long col = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (col >= c.ncols) return;
-  const int Ln = c.L[c.nu];
+  const int Ln = c.Lnu;
   Mat<N, double> O = mident<N, double>();
   for (int b = 0; b < Ln; ++b) {
     om.store(col * Ln + b, O);
@@ -147,7 +153,7 @@ __global__ void __launch_bounds__(128) uprime_kernel(Links<N, T> U, Geom g, ColG
   if (t >= c.ncols * c.rows) return;
   const long long col = t / c.rows;
   const int row = (int)(t - col * c.rows);
-  const int Ln = c.L[c.nu];
+  const int Ln = c.Lnu;
   const int b = row % Ln, k = row / Ln;
   const long long cp = col_shift(c, col, 1);
   const Mat<N, T> u = U.load(site_lin(g, col_site(c, col, b)), c.mu);
@@ -165,10 +171,18 @@ __global__ void __launch_bounds__(128) uprime_kernel(Links<N, T> U, Geom g, ColG
 constexpr int WL_THREADS = 128;
 constexpr int WL_WARPS = WL_THREADS / 32;
 
+// The (L, T) pair list of one launch, in the kernel parameters: entries
+// off[L] .. off[L+1]-1 are the loops of spatial length L, with temporal extent
+// T[k] and pair index p[k].  Up to WL_MAXP pairs and loop lengths.
 struct WLTable {
   int lmax, tmax, npairs;
   int R, CW, ntile_rows;
   long long ntiles;
+  short off[WL_MAXP + 2];
+  short T[WL_MAXP];
+  short p[WL_MAXP];
+  // bit k: entries k .. k+7 have the same L and T[k+j] = T[k] + j
+  uint32_t run8[WL_MAXP / 32];
 };
 
 // Sum of v[0..7] over the warp: on return lanes with (lane & 3) == 0 hold the
@@ -195,91 +209,209 @@ KLFT_D double warp_transpose_sum8(double v[8], int lane) {
   return y;
 }
 
-// Loops for all requested (L, T): tab_off[L]..tab_off[L+1] index tab_T / tab_p.
-template <typename T> struct WLMinBlocks { static constexpr int v = 4; };
+#ifndef KLFT_WL_MINB_F32
+#define KLFT_WL_MINB_F32 4
+#endif
+template <typename T> struct WLMinBlocks { static constexpr int v = KLFT_WL_MINB_F32; };
 template <> struct WLMinBlocks<double> { static constexpr int v = 2; };
 
+// Shared tile entries are records of N*N complex numbers padded to a multiple of
+// 16 bytes with an odd number of 16-byte units, so that 8 consecutive entries
+// read with 16-byte loads fall in distinct bank groups (float SU(3): 80 B,
+// double SU(3): 144 B).
+template <int N, typename T> struct TileEnt {
+  static constexpr int raw = N * N * (int)sizeof(cx<T>);
+  static constexpr int r16 = (raw + 15) / 16 * 16;
+  static constexpr int bytes = (r16 / 16) % 2 == 1 ? r16 : r16 + 16;
+};
+
+// Within a column's block of RT entries, even rows come first and odd rows
+// after them, so that the threads of a column (which own rows 2q, 2q+1) touch
+// consecutive entries: column slot of row r = (r & 1) * ((RT + 1) / 2) + (r >> 1).
+KLFT_D int col_slot(int r, int half) { return (r & 1) * half + (r >> 1); }
+
 template <int N, typename T>
-__global__ void __launch_bounds__(WL_THREADS, WLMinBlocks<T>::v) wloop_kernel(CField<N, T> up, ColGeom c, WLTable w,
-                                                           const int *__restrict__ tab_off,
-                                                           const int *__restrict__ tab_T,
-                                                           const int *__restrict__ tab_p, double *part) {
+KLFT_D void tile_store(unsigned char *S, int e, const Mat<N, T> &m) {
+  cx<T> *q = (cx<T> *)(S + (size_t)e * TileEnt<N, T>::bytes);
+#pragma unroll
+  for (int k = 0; k < N * N; ++k) q[k] = m.e[k / N][k % N];
+}
+template <int N, typename T>
+KLFT_D Mat<N, T> tile_load(const unsigned char *S, int e) {
+  const cx<T> *q = (const cx<T> *)(S + (size_t)e * TileEnt<N, T>::bytes);
+  Mat<N, T> m;
+#pragma unroll
+  for (int k = 0; k < N * N; ++k) m.e[k / N][k % N] = q[k];
+  return m;
+}
+// Re Tr(a b^+) with b the tile entry e, in the link precision: Sum Re(a_k conj(b_k)).
+template <int N, typename T>
+KLFT_D T tile_trace(const Mat<N, T> &a, const unsigned char *S, int e) {
+  const unsigned char *q = S + (size_t)e * TileEnt<N, T>::bytes;
+  T t = T(0);
+  if constexpr (sizeof(T) == 4 && (N * N) % 2 == 1) {
+    // 16-byte loads of complex pairs, then the odd last one
+#pragma unroll
+    for (int k = 0; k + 1 < N * N; k += 2) {
+      const float4 v = *(const float4 *)(q + 8 * k);
+      t = fma(a.e[k / N][k % N].re, v.x, t);
+      t = fma(a.e[k / N][k % N].im, v.y, t);
+      t = fma(a.e[(k + 1) / N][(k + 1) % N].re, v.z, t);
+      t = fma(a.e[(k + 1) / N][(k + 1) % N].im, v.w, t);
+    }
+    const float2 v = *(const float2 *)(q + 8 * (N * N - 1));
+    t = fma(a.e[N - 1][N - 1].re, v.x, t);
+    t = fma(a.e[N - 1][N - 1].im, v.y, t);
+  } else {
+#pragma unroll
+    for (int k = 0; k < N * N; ++k) {
+      const cx<T> v = ((const cx<T> *)q)[k];
+      t = fma(a.e[k / N][k % N].re, v.re, t);
+      t = fma(a.e[k / N][k % N].im, v.im, t);
+    }
+  }
+  return t;
+}
+
+// Re Tr(a b^+) and Re Tr(c b^+) for one tile entry b, loaded once.
+template <int N, typename T>
+KLFT_D void tile_trace2(const Mat<N, T> &a, const Mat<N, T> &c, const unsigned char *S, int e, T &ta, T &tc) {
+  const unsigned char *q = S + (size_t)e * TileEnt<N, T>::bytes;
+  if constexpr (sizeof(T) == 4 && (N * N) % 2 == 1) {
+#pragma unroll
+    for (int k = 0; k + 1 < N * N; k += 2) {
+      const float4 v = *(const float4 *)(q + 8 * k);
+      ta = fma(a.e[k / N][k % N].re, v.x, ta);
+      ta = fma(a.e[k / N][k % N].im, v.y, ta);
+      ta = fma(a.e[(k + 1) / N][(k + 1) % N].re, v.z, ta);
+      ta = fma(a.e[(k + 1) / N][(k + 1) % N].im, v.w, ta);
+      tc = fma(c.e[k / N][k % N].re, v.x, tc);
+      tc = fma(c.e[k / N][k % N].im, v.y, tc);
+      tc = fma(c.e[(k + 1) / N][(k + 1) % N].re, v.z, tc);
+      tc = fma(c.e[(k + 1) / N][(k + 1) % N].im, v.w, tc);
+    }
+    const float2 v = *(const float2 *)(q + 8 * (N * N - 1));
+    ta = fma(a.e[N - 1][N - 1].re, v.x, ta);
+    ta = fma(a.e[N - 1][N - 1].im, v.y, ta);
+    tc = fma(c.e[N - 1][N - 1].re, v.x, tc);
+    tc = fma(c.e[N - 1][N - 1].im, v.y, tc);
+  } else {
+#pragma unroll
+    for (int k = 0; k < N * N; ++k) {
+      const cx<T> v = ((const cx<T> *)q)[k];
+      ta = fma(a.e[k / N][k % N].re, v.re, ta);
+      ta = fma(a.e[k / N][k % N].im, v.im, ta);
+      tc = fma(c.e[k / N][k % N].re, v.re, tc);
+      tc = fma(c.e[k / N][k % N].im, v.im, tc);
+    }
+  }
+}
+
+// Persistent CTAs over tiles of CW columns x R rows; each thread owns two
+// consecutive origin rows of a column.  The shared tile holds, per column, the R
+// origin rows followed by T_max halo rows, so the partner of the origin at tile
+// row r for extent T is entry r + T of the same column.  For a run of eight
+// consecutive T the two origins share partners: 10 entry loads serve 16 traces.
+template <int N, typename T>
+__global__ void __launch_bounds__(WL_THREADS, WLMinBlocks<T>::v)
+    wloop_kernel(CField<N, T> up, ColGeom c, const __grid_constant__ WLTable w, double *part) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int E = w.CW * (w.R + w.tmax);  // entries: origins first, then halo rows
-  double *acc = (double *)smem_raw;                          // [npairs][WL_WARPS]
-  cx<T> *S = (cx<T> *)(acc + (size_t)w.npairs * WL_WARPS);  // [N*N][E]
+  const int RT = w.R + w.tmax;
+  const int half = (RT + 1) / 2;  // entries per row parity in a column block
+  const int QR = w.R / 2;          // threads per column
+  double *acc = (double *)smem_raw;                                                 // [npairs][WL_WARPS]
+  unsigned char *S = smem_raw + (((size_t)w.npairs * WL_WARPS * sizeof(double) + 15) & ~(size_t)15);  // entries
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   for (int p = tid; p < w.npairs * WL_WARPS; p += WL_THREADS) acc[p] = 0.0;
   __syncthreads();
-  const int Ln = c.L[c.nu];
-  const int norig = w.CW * w.R;
-  // columns never straddle a warp when R divides 32: warp-level sync suffices
-  const bool warp_local = (32 % w.R) == 0;
-  const bool has_origin = tid < norig;
-  const int cc = tid / w.R, rr = tid % w.R;
+  const int Ln = c.Lnu;
+  // columns never straddle a warp when QR divides 32: warp-level sync suffices
+  const bool warp_local = (32 % QR) == 0;
+  const bool has_origin = tid < w.CW * QR;
+  const int cc = tid / QR, q = tid % QR;
+  const int ebase = cc * 2 * half;
+  const int eo0 = ebase + q, eo1 = ebase + half + q;  // slots of the origin rows 2q, 2q + 1
   for (long long tile = blockIdx.x; tile < w.ntiles; tile += gridDim.x) {
     const long long ctile = tile / w.ntile_rows;
     const int r0 = (int)(tile - ctile * w.ntile_rows) * w.R;
     const long long col = ctile * w.CW + cc;
     const bool col_ok = has_origin && col < c.ncols;
-    Mat<N, T> own;  // S'_L at (col, r0 + rr)
+    // coordinate of the column along mu; colL = column of x + (L-1) mu, stepped per L
+    const int xm = col_ok ? (int)((col / c.csmu) % c.Lmu) : 0;
+    long long colL = col;
+    int xl = xm;
+    Mat<N, T> own0, own1;  // S'_L at rows r0 + 2q and r0 + 2q + 1
     for (int L = 1; L <= w.lmax; ++L) {
-      if (col_ok) {
-        const long long colL = col_shift(c, col, L - 1);
-        // own origin entry
-        {
-          const int row = r0 + rr;
-          if (row < c.rows) {
-            const Mat<N, T> u = up.load_t(colL * c.rows + row);
-            own = L == 1 ? u : mul(own, u);
-#pragma unroll
-            for (int a = 0; a < N * N; ++a) S[a * E + tid] = own.e[a / N][a % N];
-          }
+      if (L > 1) {
+        if (++xl == c.Lmu) {
+          xl = 0;
+          colL -= (long long)(c.Lmu - 1) * c.csmu;
+        } else {
+          colL += c.csmu;
         }
-        // halo entries j = rr, rr + R, ... of this column
-        for (int j = rr; j < w.tmax; j += w.R) {
-          const int row = r0 + w.R + j;
-          const int e = norig + cc * w.tmax + j;
-          if (row >= c.rows) continue;
-          const Mat<N, T> u = up.load_t(colL * c.rows + row);
-          Mat<N, T> s;
-          if (L == 1) {
-            s = u;
-          } else {
-            Mat<N, T> prev;
-#pragma unroll
-            for (int a = 0; a < N * N; ++a) prev.e[a / N][a % N] = S[a * E + e];
-            s = mul(prev, u);
-          }
-#pragma unroll
-          for (int a = 0; a < N * N; ++a) S[a * E + e] = s.e[a / N][a % N];
+      }
+      if (col_ok) {
+        const long long cbase = colL * c.rows + r0;
+        if (r0 + 2 * q < c.rows) {
+          const Mat<N, T> u = up.load_t(cbase + 2 * q);
+          own0 = L == 1 ? u : mul(own0, u);
+          tile_store<N, T>(S, eo0, own0);
+        }
+        if (r0 + 2 * q + 1 < c.rows) {
+          const Mat<N, T> u = up.load_t(cbase + 2 * q + 1);
+          own1 = L == 1 ? u : mul(own1, u);
+          tile_store<N, T>(S, eo1, own1);
+        }
+        for (int j = q; j < w.tmax; j += QR) {
+          if (r0 + w.R + j >= c.rows) continue;
+          const int e = ebase + col_slot(w.R + j, half);
+          const Mat<N, T> u = up.load_t(cbase + w.R + j);
+          tile_store<N, T>(S, e, L == 1 ? u : mul(tile_load<N, T>(S, e), u));
         }
       }
       if (warp_local) __syncwarp(); else __syncthreads();
-      const int k0 = tab_off[L], k1 = tab_off[L + 1];
-      const bool origin_ok = col_ok && r0 + rr < Ln;
+      const int k0 = w.off[L], k1 = w.off[L + 1];
+      // Ln and R are even, so both origin rows are inside the axis or neither is
+      const bool origin_ok = col_ok && r0 + 2 * q < Ln;
       for (int kk = k0; kk < k1; kk += 8) {
-        const int cnt = k1 - kk < 8 ? k1 - kk : 8;
-        double v[8];
+        T vt[8];
+        if (kk + 8 <= k1 && ((w.run8[kk >> 5] >> (kk & 31)) & 1u)) {
+          // in two halves of four extents: partner rows 2q + t0 + 4 hf + i, i = 0..4, of
+          // which origin 0 takes i = 0..3 and origin 1 takes i = 1..4
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-          v[j] = 0.0;
-          if (origin_ok && j < cnt) {
-            const int rr2 = rr + tab_T[kk + j];
-            const int e2 = rr2 < w.R ? cc * w.R + rr2 : norig + cc * w.tmax + (rr2 - w.R);
-            // the trace of one loop in the link precision
-            T t = T(0);
+          for (int hf = 0; hf < 2; ++hf) {
+            const int rp = 2 * q + w.T[kk] + 4 * hf;
+            T a[4], b[4];
 #pragma unroll
-            for (int a = 0; a < N * N; ++a) {
-              const cx<T> o = own.e[a / N][a % N], q = S[a * E + e2];
-              t += o.re * q.re + o.im * q.im;
+            for (int j = 0; j < 4; ++j) a[j] = b[j] = T(0);
+            if (origin_ok) {
+              a[0] = tile_trace<N, T>(own0, S, ebase + col_slot(rp, half));
+#pragma unroll
+              for (int i = 1; i < 4; ++i)
+                tile_trace2<N, T>(own0, own1, S, ebase + col_slot(rp + i, half), a[i], b[i - 1]);
+              b[3] = tile_trace<N, T>(own1, S, ebase + col_slot(rp + 4, half));
             }
-            v[j] = (double)t;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) vt[4 * hf + j] = a[j] + b[j];
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            T t = T(0);
+            if (origin_ok && kk + j < k1) {
+              const int rp = 2 * q + w.T[kk + j];
+              t = tile_trace<N, T>(own0, S, ebase + col_slot(rp, half)) +
+                  tile_trace<N, T>(own1, S, ebase + col_slot(rp + 1, half));
+            }
+            vt[j] = t;
           }
         }
+        double v[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) v[j] = (double)vt[j];
         const double tot = warp_transpose_sum8(v, lane);
         const int j = (lane >> 2) & 7;
-        if ((lane & 3) == 0 && j < cnt) acc[tab_p[kk + j] * WL_WARPS + warp] += tot;
+        if ((lane & 3) == 0 && kk + j < k1) acc[w.p[kk + j] * WL_WARPS + warp] += tot;
       }
       if (warp_local) __syncwarp(); else __syncthreads();
     }
@@ -289,7 +421,7 @@ __global__ void __launch_bounds__(WL_THREADS, WLMinBlocks<T>::v) wloop_kernel(CF
   for (int p = tid; p < w.npairs; p += WL_THREADS) {
     double s = 0.0;
 #pragma unroll
-    for (int q = 0; q < WL_WARPS; ++q) s += acc[p * WL_WARPS + q];
+    for (int q2 = 0; q2 < WL_WARPS; ++q2) s += acc[p * WL_WARPS + q2];
     part[(long long)p * gridDim.x + blockIdx.x] = s;
   }
 }
@@ -303,17 +435,23 @@ size_t wilson_gf_scratch(int nc, int dtype, const Geom &g, int nu, int tmax) {
   return al(es * g.V) + al(es * ncols) + al(es * ncols * rows);
 }
 
+// R origin rows per column tile (even: each thread owns two), CW columns per CTA.
 static void tile_shape(const Geom &g, int nu, int &R, int &CW) {
   const int Ln = g.L[nu];
   R = Ln < 32 ? Ln : 32;
-  CW = WL_THREADS / R;
+  CW = WL_THREADS / (R / 2);
+}
+
+static size_t tile_entry_bytes(int nc, int dtype) {
+  if (dtype == 0) return nc == 1 ? TileEnt<1, double>::bytes : nc == 2 ? TileEnt<2, double>::bytes : TileEnt<3, double>::bytes;
+  return nc == 1 ? TileEnt<1, float>::bytes : nc == 2 ? TileEnt<2, float>::bytes : TileEnt<3, float>::bytes;
 }
 
 size_t wilson_gf_smem(int nc, int dtype, const Geom &g, int nu, int tmax, int npairs) {
-  const size_t es = (dtype == 0 ? 16 : 8) * (size_t)nc * nc;
   int R, CW;
   tile_shape(g, nu, R, CW);
-  return (size_t)npairs * WL_WARPS * sizeof(double) + es * (size_t)CW * (R + tmax);
+  return (((size_t)npairs * WL_WARPS * sizeof(double) + 15) & ~(size_t)15) +
+         tile_entry_bytes(nc, dtype) * (size_t)CW * (2 * ((R + tmax + 1) / 2));
 }
 
 int wilson_gf_blocks(const Geom &g) {
@@ -329,7 +467,7 @@ int wilson_gf_blocks(const Geom &g) {
 }
 
 template <int N, typename T>
-static cudaError_t wilson_gf_t(const void *links, const Geom &g, const int *const *d_tab, int lmax, int tmax,
+static cudaError_t wilson_gf_t(const void *links, const Geom &g, const int *const *h_tab, int lmax, int tmax,
                                int npairs, int mu, int nu, bool omega_ready, void *scratch, double *d_part, int nblk,
                                cudaStream_t st) {
   auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
@@ -343,27 +481,39 @@ static cudaError_t wilson_gf_t(const void *links, const Geom &g, const int *cons
   Links<N, T> U{(cx<T> *)links, g.V};
   if (!omega_ready) omega_kernel<N, T><<<(unsigned)((c.ncols + 127) / 128), 128, 0, st>>>(U, g, c, om, pol);
   uprime_kernel<N, T><<<(unsigned)((c.ncols * c.rows + 127) / 128), 128, 0, st>>>(U, g, c, om, pol, up);
+  if (npairs > WL_MAXP || lmax > WL_MAXP || tmax > 32767) return cudaErrorInvalidValue;
   WLTable w;
+  std::memset(&w, 0, sizeof w);
   w.lmax = lmax;
   w.tmax = tmax;
   w.npairs = npairs;
+  for (int L = 0; L <= lmax + 1; ++L) w.off[L] = (short)h_tab[0][L];
+  for (int k = 0; k < npairs; ++k) {
+    w.T[k] = (short)h_tab[1][k];
+    w.p[k] = (short)h_tab[2][k];
+  }
+  for (int L = 1; L <= lmax; ++L)
+    for (int k = h_tab[0][L]; k + 8 <= h_tab[0][L + 1]; ++k) {
+      bool run = true;
+      for (int j = 1; j < 8; ++j) run = run && h_tab[1][k + j] == h_tab[1][k] + j;
+      if (run) w.run8[k >> 5] |= 1u << (k & 31);
+    }
   tile_shape(g, nu, w.R, w.CW);
   w.ntile_rows = (g.L[nu] + w.R - 1) / w.R;
   w.ntiles = ((c.ncols + w.CW - 1) / w.CW) * w.ntile_rows;
-  const size_t smem = (size_t)npairs * WL_WARPS * sizeof(double) + es * (size_t)w.CW * (w.R + tmax);
+  const size_t smem = (((size_t)npairs * WL_WARPS * sizeof(double) + 15) & ~(size_t)15) +
+                      (size_t)TileEnt<N, T>::bytes * w.CW * (2 * ((w.R + tmax + 1) / 2));
   cudaFuncSetAttribute(wloop_kernel<N, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-  wloop_kernel<N, T><<<nblk, WL_THREADS, smem, st>>>(up, c, w, d_tab[0], d_tab[1], d_tab[2], d_part);
+  wloop_kernel<N, T><<<nblk, WL_THREADS, smem, st>>>(up, c, w, d_part);
   return cudaGetLastError();
 }
 
 cudaError_t launch_wilson_gf(int nc, int dtype, const void *links, const Geom &g, int mu, int nu,
-                             const int *const *d_tab, const int *h_off, int lmax, int tmax, int npairs,
-                             bool omega_ready, void *scratch, double *d_part, int nblk, double *d_out,
-                             cudaStream_t st) {
-  (void)h_off;
+                             const int *const *h_tab, int lmax, int tmax, int npairs, bool omega_ready,
+                             void *scratch, double *d_part, int nblk, double *d_out, cudaStream_t st) {
   cudaError_t e = cudaErrorInvalidValue;
 #define KLFT_WGF(NV, TV) \
-  e = wilson_gf_t<NV, TV>(links, g, d_tab, lmax, tmax, npairs, mu, nu, omega_ready, scratch, d_part, nblk, st)
+  e = wilson_gf_t<NV, TV>(links, g, h_tab, lmax, tmax, npairs, mu, nu, omega_ready, scratch, d_part, nblk, st)
   if (dtype == 0) {
     if (nc == 1) KLFT_WGF(1, double);
     else if (nc == 2) KLFT_WGF(2, double);
