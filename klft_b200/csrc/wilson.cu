@@ -21,9 +21,9 @@
 // memory together with a halo of T_max rows of the same column; per-site traces
 // in the link precision, lattice sums in FP64).
 //
-// Omega and U' are stored "column major": entry (column c, row b) at c*rows + b,
-// one plane per complex colour entry, so a warp covering consecutive rows of
-// one column reads contiguous memory.
+// Omega is stored row major (row b, column c at b*ncols + c) and U' column major
+// (c*rows + b), one plane per complex colour entry: the kernels that write them
+// run lanes over columns, the loop kernel reads U' with lanes over rows.
 #include <cstring>
 
 #include "common.cuh"
@@ -130,7 +130,9 @@ template <int N, typename T> KLFT_D Mat<N, double> to_d(const Mat<N, T> &m) {
   return r;
 }
 
-// Omega(col, b) for b < L_nu, and P(col) = Omega(col, L_nu); one thread per column.
+// Omega(col, b) for b < L_nu, stored row major (b * ncols + col), and
+// P(col) = Omega(col, L_nu); one thread per column, lanes over consecutive
+// columns so that the U_nu loads and the Omega stores are coalesced.
 template <int N, typename T>
 __global__ void omega_kernel(Links<N, T> U, Geom g, ColGeom c, CField<N, T> om, CField<N, T> pol) {
   const long long col = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -138,34 +140,49 @@ __global__ void omega_kernel(Links<N, T> U, Geom g, ColGeom c, CField<N, T> om, 
   const int Ln = c.Lnu;
   Mat<N, double> O = mident<N, double>();
   for (int b = 0; b < Ln; ++b) {
-    om.store(col * Ln + b, O);
+    om.store((long long)b * c.ncols + col, O);
     O = mul(O, to_d(U.load(site_lin(g, col_site(c, col, b)), c.nu)));
   }
   pol.store(col, O);
 }
 
-// U'_mu(col, row) for row < rows; one thread per entry, rows fastest.  The
-// products run in the link precision (Omega itself is an FP64 product).
+// U'_mu(col, row) for row < rows, over tiles of 32 consecutive columns x UP_RB
+// rows: computed with lanes over columns (coalesced U and Omega reads), staged
+// in shared memory and written column major (col * rows + row) with consecutive
+// threads on consecutive rows.  The products run in the link precision (Omega
+// itself is an FP64 product).
+constexpr int UP_RB = 8;
 template <int N, typename T>
-__global__ void __launch_bounds__(128) uprime_kernel(Links<N, T> U, Geom g, ColGeom c, CField<N, T> om,
-                                                     CField<N, T> pol, CField<N, T> up) {
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= c.ncols * c.rows) return;
-  const long long col = t / c.rows;
-  const int row = (int)(t - col * c.rows);
+__global__ void __launch_bounds__(32 * UP_RB) uprime_kernel(Links<N, T> U, Geom g, ColGeom c, CField<N, T> om,
+                                                            CField<N, T> pol, CField<N, T> up) {
+  __shared__ cx<T> tile[N * N][UP_RB][33];
+  const long long nct = (c.ncols + 31) / 32;
+  const long long ctile = blockIdx.x % nct;
+  const int row0 = (int)(blockIdx.x / nct) * UP_RB;
+  const int cl = threadIdx.x & 31, r = threadIdx.x >> 5;
+  const long long col = ctile * 32 + cl;
+  const int row = row0 + r;
   const int Ln = c.Lnu;
-  const int b = row % Ln, k = row / Ln;
-  const long long cp = col_shift(c, col, 1);
-  const Mat<N, T> u = U.load(site_lin(g, col_site(c, col, b)), c.mu);
-  Mat<N, T> v = mul_nd(mul(om.load_t(col * Ln + b), u), om.load_t(cp * Ln + b));
-  if (k > 0) {
-    const Mat<N, T> P = pol.load_t(col), Pp = pol.load_t(cp);
-    for (int i = 0; i < k; ++i) v = mul_nd(mul(P, v), Pp);
+  if (col < c.ncols && row < c.rows) {
+    const int b = row % Ln, k = row / Ln;
+    const long long cp = col_shift(c, col, 1);
+    const Mat<N, T> u = U.load(site_lin(g, col_site(c, col, b)), c.mu);
+    Mat<N, T> v = mul_nd(mul(om.load_t((long long)b * c.ncols + col), u), om.load_t((long long)b * c.ncols + cp));
+    if (k > 0) {
+      const Mat<N, T> P = pol.load_t(col), Pp = pol.load_t(cp);
+      for (int i = 0; i < k; ++i) v = mul_nd(mul(P, v), Pp);
+    }
+#pragma unroll
+    for (int a = 0; a < N * N; ++a) tile[a][r][cl] = v.e[a / N][a % N];
   }
+  __syncthreads();
+  const int cl2 = threadIdx.x / UP_RB, r2 = threadIdx.x % UP_RB;
+  const long long col2 = ctile * 32 + cl2;
+  const int row2 = row0 + r2;
+  if (col2 < c.ncols && row2 < c.rows) {
 #pragma unroll
-  for (int a = 0; a < N; ++a)
-#pragma unroll
-    for (int bb = 0; bb < N; ++bb) up.p[(a * N + bb) * up.n + t] = v.e[a][bb];
+    for (int a = 0; a < N * N; ++a) up.p[(long long)a * up.n + col2 * c.rows + row2] = tile[a][r2][cl2];
+  }
 }
 
 constexpr int WL_THREADS = 128;
@@ -480,7 +497,9 @@ static cudaError_t wilson_gf_t(const void *links, const Geom &g, const int *cons
   CField<N, T> up{(cx<T> *)(base + al(es * Vc) + al(es * c.ncols)), c.ncols * c.rows};
   Links<N, T> U{(cx<T> *)links, g.V};
   if (!omega_ready) omega_kernel<N, T><<<(unsigned)((c.ncols + 127) / 128), 128, 0, st>>>(U, g, c, om, pol);
-  uprime_kernel<N, T><<<(unsigned)((c.ncols * c.rows + 127) / 128), 128, 0, st>>>(U, g, c, om, pol, up);
+  const long long nct = (c.ncols + 31) / 32;
+  uprime_kernel<N, T><<<(unsigned)(nct * ((c.rows + UP_RB - 1) / UP_RB)), 32 * UP_RB, 0, st>>>(U, g, c, om, pol,
+                                                                                             up);
   if (npairs > WL_MAXP || lmax > WL_MAXP || tmax > 32767) return cudaErrorInvalidValue;
   WLTable w;
   std::memset(&w, 0, sizeof w);
