@@ -11,9 +11,8 @@ constexpr double K2PI = 6.283185307179586;
 enum Proposal : int { PROPOSAL_REFERENCE = 0, PROPOSAL_EXP = 1 };
 
 // ------------------------------------------------------------------ SU(3) exponential
-// exp(iQ) for hermitian traceless 3x3 Q by the Cayley-Hamilton form of
-// Morningstar & Peardon, Phys. Rev. D 69 (2004) 054501, eqs. (23)-(34):
-// exp(iQ) = f0 + f1 Q + f2 Q^2 with the f_j from c0 = det Q, c1 = Tr Q^2 / 2.
+// exp(iQ) for hermitian traceless 3x3 Q in the Cayley-Hamilton basis
+// (1, Q, Q^2) (cf. Morningstar & Peardon, Phys. Rev. D 69 (2004) 054501).
 // Q^2 of a hermitian Q: the upper triangle, mirrored.
 template <typename T> KLFT_D Mat<3, T> herm_square(const Mat<3, T> &Q) {
   Mat<3, T> Q2;
@@ -35,73 +34,71 @@ template <typename T> KLFT_D Mat<3, T> herm_square(const Mat<3, T> &Q) {
   return Q2;
 }
 
-// Fast single-precision functions for the mixed form.  The arguments of the
-// SU(3) exponential are bounded (|x| <= pi), where the SFU forms are accurate
-// to about 1e-6 absolute, the round-off level of FP32 links.
-struct FastMath {
-  static KLFT_D float fsin(float x) { return __sinf(x); }
-  static KLFT_D float fcos(float x) { return __cosf(x); }
-  static KLFT_D float frsqrt(float x) { return rsqrtf(x); }
-  static KLFT_D float frcp(float x) { return __fdividef(1.0f, x); }
-  static KLFT_D double fsin(double x) { return sin(x); }
-  static KLFT_D double fcos(double x) { return cos(x); }
-  static KLFT_D double frsqrt(double x) { return 1.0 / sqrt(x); }
-  static KLFT_D double frcp(double x) { return 1.0 / x; }
-};
+// exp(iQ) = f0 + f1 Q + f2 Q^2 for hermitian traceless 3x3 Q, with the f_j
+// summed in coefficient space.  Cayley-Hamilton gives Q^3 = c1 Q + c0 with
+// c1 = Tr Q^2 / 2 and c0 = det Q (real), so every power Q^n = a_n + b_n Q + d_n Q^2
+// with the real recurrence (a, b, d)_{n+1} = (d c0, a + d c1, b), and
+// f = sum_n i^n/n! (a_n, b_n, d_n).  Arguments with c1 > 3/4 (an eigenvalue
+// possibly above 1: |lambda|^2 <= 4 c1 / 3) are scaled by 2^-s and the result
+// squared s times, also in coefficient space:
+//   (f0 + f1 Q + f2 Q^2)^2 = (f0^2 + 2 f1 f2 c0) + (2 f0 f1 + 2 f1 f2 c1 + f2^2 c0) Q
+//                          + (f1^2 + 2 f0 f2 + f2^2 c1) Q^2.
+// Terms: 12 in FP32 and 19 in FP64 (|lambda| <= 1: 1/12! < 3e-9, 1/19! < 1e-17).
+template <typename T> struct ExpTerms { static constexpr int n = 12; };
+template <> struct ExpTerms<double> { static constexpr int n = 19; };
 
 template <typename T> KLFT_D Mat<3, T> expi_su3(const Mat<3, T> &Q) {
   const Mat<3, T> Q2 = herm_square(Q);
-  const T c1 = T(0.5) * (Q2.e[0][0].re + Q2.e[1][1].re + Q2.e[2][2].re);
+  T c1 = T(0.5) * (Q2.e[0][0].re + Q2.e[1][1].re + Q2.e[2][2].re);
   // c0 = det Q, real for hermitian Q
-  const T c0 = Q.e[0][0].re * (Q.e[1][1].re * Q.e[2][2].re - (Q.e[1][2].re * Q.e[1][2].re + Q.e[1][2].im * Q.e[1][2].im)) -
-               Q.e[1][1].re * (Q.e[0][2].re * Q.e[0][2].re + Q.e[0][2].im * Q.e[0][2].im) -
-               Q.e[2][2].re * (Q.e[0][1].re * Q.e[0][1].re + Q.e[0][1].im * Q.e[0][1].im) +
-               T(2) * (Q.e[0][1] * Q.e[1][2] * Q.e[2][0]).re;
-  cx<T> f0, f1, f2;
-  const T tiny = sizeof(T) == 8 ? T(1e-16) : T(1e-10);
-  if (c1 < tiny) {
-    // series: exp(iQ) ~ 1 + iQ - Q^2/2 (Q^3 term is O(c1^{3/2}) below tiny)
-    f0 = mk<T>(T(1), T(0));
-    f1 = mk<T>(T(0), T(1));
-    f2 = mk<T>(T(-0.5), T(0));
-  } else {
-    const bool neg = c0 < T(0);
-    const T ac0 = neg ? -c0 : c0;
-    // with r = (c1/3)^(-1/2): sqrt(c1/3) = (c1/3) r, c0max = 2 (c1/3)^(3/2)
-    const T c13 = c1 * T(1.0 / 3.0);
-    const T r = FastMath::frsqrt(c13);
-    const T s13 = c13 * r;
-    T ratio = T(0.5) * ac0 * (r * r * r);
-    ratio = ratio > T(1) ? T(1) : ratio;
-    const T theta = acos(ratio);
-    const T u = s13 * FastMath::fcos(theta * T(1.0 / 3.0));
-    const T w = T(1.7320508075688772) * s13 * FastMath::fsin(theta * T(1.0 / 3.0));
-    const T u2 = u * u, w2 = w * w;
-    T xi0;
-    if (fabs(w) < T(0.05)) {
-      xi0 = T(1) - w2 * T(1.0 / 6.0) * (T(1) - w2 * T(1.0 / 20.0) * (T(1) - w2 * T(1.0 / 42.0)));
+  T c0 = Q.e[0][0].re * (Q.e[1][1].re * Q.e[2][2].re - (Q.e[1][2].re * Q.e[1][2].re + Q.e[1][2].im * Q.e[1][2].im)) -
+         Q.e[1][1].re * (Q.e[0][2].re * Q.e[0][2].re + Q.e[0][2].im * Q.e[0][2].im) -
+         Q.e[2][2].re * (Q.e[0][1].re * Q.e[0][1].re + Q.e[0][1].im * Q.e[0][1].im) +
+         T(2) * (Q.e[0][1] * Q.e[1][2] * Q.e[2][0]).re;
+  int sq = 0;
+  T scale = T(1);
+  while (c1 > T(0.75) && sq < 64) {  // halve Q: c1 / 4, c0 / 8
+    c1 *= T(0.25);
+    c0 *= T(0.125);
+    scale *= T(0.5);
+    ++sq;
+  }
+  // Taylor sum of exp(i Q'), Q' = scale Q, in the basis (1, Q', Q'^2)
+  T a = T(1), b = T(0), d = T(0), fact = T(1);
+  cx<T> f0 = mk<T>(T(1), T(0)), f1 = mk<T>(T(0), T(0)), f2 = mk<T>(T(0), T(0));
+#pragma unroll
+  for (int n = 1; n < ExpTerms<T>::n; ++n) {
+    const T an = d * c0, bn = a + d * c1, dn = b;
+    a = an;
+    b = bn;
+    d = dn;
+    fact *= T(1) / T(n);
+    // i^n: 1, i, -1, -i
+    const T sgn = ((n >> 1) & 1) ? T(-1) : T(1);
+    if (n & 1) {
+      f0.im += sgn * fact * a;
+      f1.im += sgn * fact * b;
+      f2.im += sgn * fact * d;
     } else {
-      xi0 = FastMath::fsin(w) * FastMath::frcp(w);
-    }
-    const T cw = FastMath::fcos(w);
-    const T s2u = FastMath::fsin(T(2) * u), c2u = FastMath::fcos(T(2) * u);
-    const T smu = -FastMath::fsin(u), cmu = FastMath::fcos(u);
-    const cx<T> e2iu = mk<T>(c2u, s2u);
-    const cx<T> emiu = mk<T>(cmu, smu);
-    const cx<T> h0 = e2iu * (u2 - w2) + emiu * mk<T>(T(8) * u2 * cw, T(2) * u * (T(3) * u2 + w2) * xi0);
-    const cx<T> h1 = e2iu * (T(2) * u) - emiu * mk<T>(T(2) * u * cw, -(T(3) * u2 - w2) * xi0);
-    const cx<T> h2 = e2iu - emiu * mk<T>(cw, T(3) * u * xi0);
-    // 9u^2 - w^2 = c1 (3 cos^2(theta/3) - sin^2(theta/3)) >= 2 c1 for theta in [0, pi/2]
-    const T iden = FastMath::frcp(T(9) * u2 - w2);
-    f0 = mk<T>(h0.re * iden, h0.im * iden);
-    f1 = mk<T>(h1.re * iden, h1.im * iden);
-    f2 = mk<T>(h2.re * iden, h2.im * iden);
-    if (neg) {  // f_j(-c0) = (-1)^j conj(f_j(c0))
-      f0 = conj(f0);
-      f1 = mk<T>(-f1.re, f1.im);
-      f2 = conj(f2);
+      f0.re += sgn * fact * a;
+      f1.re += sgn * fact * b;
+      f2.re += sgn * fact * d;
     }
   }
+  for (int k = 0; k < sq; ++k) {
+    const cx<T> f12 = f1 * f2, f22 = f2 * f2;
+    const cx<T> g0 = f0 * f0 + f12 * (T(2) * c0);
+    const cx<T> g1 = (f0 * f1) * T(2) + f12 * (T(2) * c1) + f22 * c0;
+    const cx<T> g2 = f1 * f1 + (f0 * f2) * T(2) + f22 * c1;
+    f0 = g0;
+    f1 = g1;
+    f2 = g2;
+    c1 *= T(4);
+    c0 *= T(8);
+  }
+  // back to the basis (1, Q, Q^2): Q' = scale Q
+  f1 = f1 * scale;
+  f2 = f2 * (scale * scale);
   Mat<3, T> R;
 #pragma unroll
   for (int i = 0; i < 3; ++i)
