@@ -144,7 +144,7 @@ klft_status klft_lattice_create(int nc, int ndims, const int *L, int precision, 
   lat->g = make_geom(ndims, L);
   const Geom &g = lat->g;
   cudaGetDevice(&lat->device);
-  lat->link_bytes = (size_t)V * ndims * nc * nc * elem_bytes(precision);
+  lat->link_bytes = (size_t)V * ndims * link_planes(nc, lat->dtype()) * elem_bytes(precision);
   e = cudaStreamCreateWithFlags(&lat->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) { delete lat; return cuda_fail(e, "cudaStreamCreate"); }
   e = cudaMalloc(&lat->links, lat->link_bytes);

@@ -354,24 +354,43 @@ KLFT_HD Site site_from_lex(const Geom &g, long long lex) {
 }
 
 // ------------------------------------------------------------------ link field view
+// Stored colour planes per link: all N*N, except SU(3) in the mixed (FP32)
+// form, which keeps rows 0 and 1 (12 reals) and rebuilds row 2 as
+// conj(row0 x row1), the unit-determinant completion of two orthonormal rows.
+template <int N, typename T> struct LinkPlanes { static constexpr int n = N * N; };
+template <> struct LinkPlanes<3, float> { static constexpr int n = 6; };
+KLFT_HD int link_planes(int nc, int dtype) { return (nc == 3 && dtype == 1) ? 6 : nc * nc; }
+
 template <int N, typename T> struct Links {
   cx<T> *p;
   long long V;
+  static constexpr int P = LinkPlanes<N, T>::n;
   KLFT_D Mat<N, T> load(long long lin, int mu) const {
     Mat<N, T> m;
-    const cx<T> *q = p + (long long)mu * N * N * V + lin;
+    const cx<T> *q = p + (long long)mu * P * V + lin;
+    if constexpr (P == N * N) {
 #pragma unroll
-    for (int i = 0; i < N; ++i)
+      for (int i = 0; i < N; ++i)
 #pragma unroll
-      for (int j = 0; j < N; ++j) m.e[i][j] = q[(i * N + j) * V];
+        for (int j = 0; j < N; ++j) m.e[i][j] = q[(i * N + j) * V];
+    } else {
+#pragma unroll
+      for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) m.e[i][j] = q[(i * 3 + j) * V];
+      m.e[2][0] = conj(m.e[0][1] * m.e[1][2] - m.e[0][2] * m.e[1][1]);
+      m.e[2][1] = conj(m.e[0][2] * m.e[1][0] - m.e[0][0] * m.e[1][2]);
+      m.e[2][2] = conj(m.e[0][0] * m.e[1][1] - m.e[0][1] * m.e[1][0]);
+    }
     return m;
   }
   KLFT_D void store(long long lin, int mu, const Mat<N, T> &m) const {
-    cx<T> *q = p + (long long)mu * N * N * V + lin;
+    cx<T> *q = p + (long long)mu * P * V + lin;
 #pragma unroll
     for (int i = 0; i < N; ++i)
 #pragma unroll
-      for (int j = 0; j < N; ++j) q[(i * N + j) * V] = m.e[i][j];
+      for (int j = 0; j < N; ++j)
+        if ((i * N + j) < P) q[(i * N + j) * V] = m.e[i][j];
   }
 };
 

@@ -331,7 +331,7 @@ namespace klft {
 size_t hmc_footprint(int nc, int dtype, const Geom &g, int ntraj) {
   auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
   const size_t pb = (size_t)g.V * g.nd * ncomp_of(nc) * (dtype == 0 ? 8 : 4);
-  const size_t lb = (size_t)g.V * g.nd * nc * nc * (dtype == 0 ? 16 : 8);
+  const size_t lb = (size_t)g.V * g.nd * link_planes(nc, dtype) * (dtype == 0 ? 16 : 8);
   return al(pb) + al(lb) + al(8 * sizeof(double)) + al((size_t)ntraj * sizeof(double)) +
          al((size_t)ntraj * sizeof(int)) + (size_t)plaquette_blocks(g) * sizeof(double);
 }

@@ -138,7 +138,7 @@ klft_status validate(const klft_job *j) {
 uint64_t footprint_of(const klft_job &j) {
   const Geom g = make_geom(j.ndims, j.L);
   const int dtype = j.precision == KLFT_PRECISION_FP64 ? 0 : 1;
-  uint64_t b = (uint64_t)g.V * j.ndims * j.nc * j.nc * (dtype == 0 ? 16 : 8);  // links
+  uint64_t b = (uint64_t)g.V * j.ndims * link_planes(j.nc, dtype) * (dtype == 0 ? 16 : 8);  // links
   b += 4096 + KLFT_RESULT_SLOTS * sizeof(double);                            // counters, result slots
   b += (uint64_t)plaquette_blocks(g) * sizeof(double);
   if (j.n_wilson > 0) {
