@@ -258,6 +258,22 @@ def cpu_baseline_reference(L: int):
                       f"{dt:.2f} s"}
 
 
+# DRAM traffic of one parity pass (dram__bytes_read.sum + dram__bytes_write.sum of one
+# metropolis_exp_kernel launch in the ncu capture summarised in the profile below).
+TRAFFIC_PASS_BYTES = 113256192
+TRAFFIC_SOURCE = "profiles/metropolis_exp_su3_32x4_mixed.md"
+
+
+def sweep_flops_per_link_update(nhits: int, acceptance: float) -> float:
+    """Algorithmic flops of one SU(3) exp(i eps H) link update (6 per complex
+    multiply, 2 per complex add, 198 per 3x3 product): staple 2466, M = U S 198,
+    per hit the proposal (8 Box-Muller normals 32, Gell-Mann sum 16, Q^2 132,
+    c0/c1 30, 12-term coefficient series 108, X = f0 + f1 Q + f2 Q^2 126) + Re Tr(X M)
+    36 + acceptance x (X U, X M) 396, and one reunitarisation (~100)."""
+    proposal = 32 + 16 + 132 + 30 + 108 + 126
+    return 2466 + 198 + nhits * (proposal + 36 + acceptance * 396) + 100
+
+
 def plaquette_ms(g, eps, reps=5):
     """Device time of one GaugePlaquette (ms) from cycles with and without it."""
     _, _, _, ms_sweep = g.run_cycles(BETA, 0.0, NHITS, reps, "exp", eps, False, [])
@@ -376,15 +392,23 @@ def run_ours(a, dist: Dist):
     hbm = pk.get("hbm_gbs")
     fp32 = peak(1)
     fp64 = peak(0)
-    bytes_link_mixed = 2 * 9 * 8  # read + write one FP32 SU(3) link
+    # read + write one FP32 SU(3) link, stored as two rows (12 reals)
+    bytes_link_mixed = 2 * 6 * 8
     pass_ms = ms_sweep / 16.0
     units_per_launch = V // 16 * 4
     achieved = units_per_launch * bytes_link_mixed / (pass_ms * 1e-3) / 1e9
-    roofline = {"bound": "hbm", "kernel": "metropolis_pass_kernel<3,4,float>", "achieved": achieved,
+    flop_lu = sweep_flops_per_link_update(NHITS, float(np.mean(acc)))
+    tflops = units_per_launch * flop_lu / (pass_ms * 1e-3) / 1e12
+    roofline = {"bound": "hbm", "kernel": "metropolis_exp_kernel<4,float,false>", "achieved": achieved,
                 "peak": hbm, "unit": "GB/s", "frac": (achieved / hbm) if hbm else None,
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if hbm else "fallback 6650",
-                "traffic": None, "algorithmic_bytes_per_launch": units_per_launch * bytes_link_mixed,
-                "avg_launch_ms": pass_ms,
+                "traffic": TRAFFIC_PASS_BYTES, "traffic_source": TRAFFIC_SOURCE,
+                "algorithmic_bytes_per_launch": units_per_launch * bytes_link_mixed,
+                "units_per_launch": units_per_launch, "avg_launch_ms": pass_ms,
+                "cuda_core": {"achieved_tflops": tflops, "peak_tflops": fp32, "frac": (tflops / fp32) if fp32 else None,
+                              "flop_per_link_update": flop_lu,
+                              "peak_source": "klft_peak_flops (measured FP32 FMA throughput)",
+                              "note": "the binding roof: ~65 flop per algorithmic byte, above the FP32 ridge"},
                 "cuda_core_peak_tflops": {"fp32": fp32, "fp64": fp64}}
     e2e_dt, h2d, d2h = e2e_public_api(g, eps, max(2, a.steps // 2))
     e2e_steps = max(2, a.steps // 2)
