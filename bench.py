@@ -274,6 +274,24 @@ def sweep_flops_per_link_update(nhits: int, acceptance: float) -> float:
     return 2466 + 198 + nhits * (proposal + 36 + acceptance * 396) + 100
 
 
+def mixed_errors(g, L):
+    """Error of the mixed form per observable: the final mixed-form configuration
+    evaluated by both forms on identical links (its FP32 values are exact in FP64),
+    plus the unitarity drift max ||U^+ U - 1|| of the mixed links."""
+    import klft_b200
+    U = g.download()
+    g64 = klft_b200.GaugeField(L, 3, "fp64", "cold", 0)
+    g64.upload(U)
+    p32, p64 = g.plaquette(), g64.plaquette()
+    w32, w64 = g.wilson_loop_temporal(PAIRS), g64.wilson_loop_temporal(PAIRS)
+    out = {"plaquette_abs": abs(p32 - p64), "wilson_temporal_max_abs": float(np.max(np.abs(w32 - w64))),
+           "wilson_temporal_max_rel": float(np.max(np.abs(w32 - w64) / np.abs(w64))),
+           "unitarity_mixed": g.unitarity(),
+           "note": "same configuration, FP32 link arithmetic vs FP64; sums in FP64 in both"}
+    g64.close()
+    return out
+
+
 def plaquette_ms(g, eps, reps=5):
     """Device time of one GaugePlaquette (ms) from cycles with and without it."""
     _, _, _, ms_sweep = g.run_cycles(BETA, 0.0, NHITS, reps, "exp", eps, False, [])
@@ -431,6 +449,7 @@ def run_ours(a, dist: Dist):
         fp64_line = {"value": links_per_step * a.steps * dist.world / (ms64 * 1e-3), "ms_per_step": ms64 / a.steps,
                      "ms_sweep": s64, "ms_measure": m64, "mean_plaquette": float(np.mean(plaq64))}
         g64.close()
+    mixed_err = mixed_errors(g, L)
     launches_per_step = 16 + 1 + 2 + 3 * 2  # passes + counter advance + plaquette(2) + 3 x wilson(2)
     line = {
         "metric": METRIC, "value": value, "unit": "link updates/s", "n_gpus": dist.world, "steps": a.steps,
@@ -443,7 +462,7 @@ def run_ours(a, dist: Dist):
                    "l2": f"inputs larger than L2 ({V * 4 * 9 * 8 / 1e6:.0f} MB of FP32 links)"},
         "breakdown_ms": {"sweep": ms_sweep, "measure": ms_meas},
         "acceptance": float(np.mean(acc)), "mean_plaquette": float(np.mean(plaq)),
-        "fp64": fp64_line,
+        "fp64": fp64_line, "mixed_error": mixed_err,
         "roofline": roofline, "e2e": e2e, "e2e_host_lattice": e2e_host,
         "clocks": clocks.summary(), "gpu_launches": launches_per_step * a.steps,
     }
