@@ -72,6 +72,13 @@ klft_status klft_lattice_set_counters(klft_lattice *lat, uint32_t sweep, uint32_
 /* Copy links from / to a host buffer in the interchange layout. */
 klft_status klft_lattice_upload(klft_lattice *lat, const double *host);
 klft_status klft_lattice_download(klft_lattice *lat, double *host);
+/* Open boundary in direction mu (the intent of GaugeField.hpp:168-185 openBC<mu>,
+ * whose body indexes past the lattice and does not compile): the links U_mu on
+ * the slice x_mu = L_mu - 1 are set to zero and never updated, so every staple,
+ * plaquette and Wilson loop through them vanishes; reunitarisation and the
+ * unitarity check skip them.  Uploads re-zero them.  mu = -1 on a periodic
+ * lattice is a no-op; an open direction cannot be closed again. */
+klft_status klft_lattice_set_open_boundary(klft_lattice *lat, int mu);
 
 /* nsweeps Metropolis sweeps; acc_out[k] = acceptance of sweep k normalised as
  * sweep_Metropolis does (Metropolis.hpp:118-178).  Replaces sweep_Metropolis. */

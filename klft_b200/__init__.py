@@ -219,6 +219,10 @@ class GaugeField:
         return k.value, s.value
 
     # -- PTBC
+    def set_open_boundary(self, mu: int) -> None:
+        """Open boundary in direction mu: links across the last slice are zero and never updated."""
+        check(lib().klft_lattice_set_open_boundary(self._h, mu))
+
     def set_defect(self, length: int, pos=(0, 0, 0), c: float = 1.0) -> None:
         p = (C.c_int * 3)(*(list(pos) + [0, 0, 0])[:3])
         check(lib().klft_lattice_set_defect(self._h, length, p, c))

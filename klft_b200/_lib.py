@@ -61,6 +61,7 @@ SIGNATURES = {
     "klft_lattice_set_counters": (C.c_int, [_vp, C.c_uint32, C.c_uint32]),
     "klft_lattice_upload": (C.c_int, [_vp, _dp]),
     "klft_lattice_download": (C.c_int, [_vp, _dp]),
+    "klft_lattice_set_open_boundary": (C.c_int, [_vp, C.c_int]),
     "klft_metropolis_sweeps": (C.c_int, [_vp, C.c_double, C.c_double, C.c_int, C.c_int, C.c_double, C.c_int, _dp]),
     "klft_plaquette": (C.c_int, [_vp, _dp]),
     "klft_wilson_loop_mu_nu": (C.c_int, [_vp, C.c_int, C.c_int, _ip, C.c_int, _dp]),

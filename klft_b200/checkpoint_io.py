@@ -16,6 +16,7 @@ MAGIC = b"KLFTCKPT"
 VERSION = 1
 HEADER = 128
 _FMT = "<8sII" + "7i" + "5i" + "QQ" + "4I" + "d" + "Q" + "Q"  # up to byte 120; then the header checksum
+# the fourth u32 after the stream (byte 92) is the open-boundary direction + 1 (0: periodic)
 
 
 def fnv1a64(data: bytes) -> int:
@@ -33,7 +34,8 @@ class Checkpoint:
     precision: int  # 0 = FP64, 1 = mixed
     seed: int
     chain: int
-    counters: Tuple[int, int, int, int] = (0, 0, 0, 0)
+    counters: Tuple[int, int, int] = (0, 0, 0)
+    open_mu: int = -1
     defect_len: int = 0
     defect_pos: Tuple[int, int, int] = (0, 0, 0)
     defect_c: float = 1.0
@@ -50,7 +52,7 @@ def to_bytes(ck: Checkpoint) -> bytes:
     payload = np.ascontiguousarray(ck.links, dtype=np.complex128).tobytes()
     head = struct.pack(_FMT, MAGIC, VERSION, HEADER, ck.nc, nd, *L4, ck.precision,
                        1 if ck.defect_len > 0 else 0, ck.defect_len, *ck.defect_pos, ck.seed, ck.chain,
-                       *ck.counters, ck.defect_c, len(payload), fnv1a64(payload))
+                       *ck.counters, ck.open_mu + 1, ck.defect_c, len(payload), fnv1a64(payload))
     assert len(head) == 120
     head += struct.pack("<Q", fnv1a64(head))
     return head + payload
@@ -67,7 +69,7 @@ def read(path: str) -> Checkpoint:
     if len(data) < HEADER:
         raise ValueError("short header")
     vals = struct.unpack(_FMT, data[:120])
-    (magic, ver, hb, nc, nd, l0, l1, l2, l3, prec, dact, dlen, p0, p1, p2, seed, chain, c0, c1, c2, c3, dc,
+    (magic, ver, hb, nc, nd, l0, l1, l2, l3, prec, dact, dlen, p0, p1, p2, seed, chain, c0, c1, c2, open1, dc,
      nbytes, csum) = vals
     if magic != MAGIC:
         raise ValueError("not a checkpoint")
@@ -83,5 +85,6 @@ def read(path: str) -> Checkpoint:
     L = [l0, l1, l2, l3][:nd]
     V = int(np.prod(L))
     links = np.frombuffer(payload, dtype=np.complex128).reshape(V, nd, nc, nc).copy()
-    return Checkpoint(nc=nc, L=L, precision=prec, seed=seed, chain=chain, counters=(c0, c1, c2, c3),
-                      defect_len=dlen if dact else 0, defect_pos=(p0, p1, p2), defect_c=dc, links=links)
+    return Checkpoint(nc=nc, L=L, precision=prec, seed=seed, chain=chain, counters=(c0, c1, c2),
+                      open_mu=open1 - 1, defect_len=dlen if dact else 0, defect_pos=(p0, p1, p2), defect_c=dc,
+                      links=links)

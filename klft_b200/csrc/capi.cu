@@ -95,6 +95,7 @@ Geom make_geom(int ndims, const int *L) {
   }
   g.V = V;
   g.Vh = Vh;
+  g.open_mu = -1;
   return g;
 }
 }  // namespace klft
@@ -233,6 +234,23 @@ klft_status klft_lattice_upload(klft_lattice *lat, const double *host) {
   CK(lat->s_stage.ensure(bytes));
   CK(cudaMemcpyAsync(lat->s_stage.ptr, host, bytes, cudaMemcpyHostToDevice, lat->stream));
   CK(launch_import(lat->nc, lat->dtype(), lat->links, lat->g, (const double *)lat->s_stage.ptr, lat->stream));
+  CK(launch_open_boundary(lat->nc, lat->dtype(), lat->links, lat->g, lat->stream));
+  CK(cudaStreamSynchronize(lat->stream));
+  return KLFT_OK;
+}
+
+klft_status klft_lattice_set_open_boundary(klft_lattice *lat, int mu) {
+  if (!lat) return fail(KLFT_EINVAL, "klft_lattice_set_open_boundary: null handle");
+  if (mu < -1 || mu >= lat->g.nd)
+    return fail(KLFT_EINVAL, "klft_lattice_set_open_boundary: direction %d outside -1..%d", mu, lat->g.nd - 1);
+  LOCK(lat);
+  if (mu < 0 && lat->g.open_mu >= 0)
+    return fail(KLFT_EINVAL, "klft_lattice_set_open_boundary: the zeroed boundary links cannot be restored; "
+                             "upload a configuration into a new lattice instead");
+  if (mu >= 0 && lat->g.open_mu >= 0 && mu != lat->g.open_mu)
+    return fail(KLFT_EINVAL, "klft_lattice_set_open_boundary: direction %d is already open", lat->g.open_mu);
+  lat->g.open_mu = mu;
+  CK(launch_open_boundary(lat->nc, lat->dtype(), lat->links, lat->g, lat->stream));
   CK(cudaStreamSynchronize(lat->stream));
   return KLFT_OK;
 }

@@ -13,7 +13,8 @@
 //  16  i32      Nc, ndims, L[4], precision          (7 x 4 B)
 //  44  i32      defect active, len, pos[3]          (5 x 4 B)
 //  64  u64      seed, chain
-//  80  u32      counters[4] (sweep, trajectory, cycle, spare)
+//  80  u32      counters[3] (sweep, trajectory, cycle)
+//  92  u32      open-boundary direction + 1 (0: periodic)
 //  96  f64      defect coefficient
 // 104  u64      payload bytes
 // 112  u64      FNV-1a 64 of the payload
@@ -74,6 +75,7 @@ klft_status klft_checkpoint_write(klft_lattice *lat, const char *path) {
   uint32_t ctr[4];
   Defect df;
   uint64_t seed, chain;
+  int open_mu;
   {
     std::lock_guard<std::mutex> g(lat->mtx);
     cudaError_t e = cudaMemcpyAsync(ctr, lat->d_counters, sizeof ctr, cudaMemcpyDeviceToHost, lat->stream);
@@ -82,6 +84,7 @@ klft_status klft_checkpoint_write(klft_lattice *lat, const char *path) {
     df = lat->defect;
     seed = lat->seed;
     chain = lat->chain;
+    open_mu = lat->g.open_mu;
   }
   unsigned char h[kHeader];
   std::memset(h, 0, sizeof h);
@@ -97,7 +100,8 @@ klft_status klft_checkpoint_write(klft_lattice *lat, const char *path) {
   for (int k = 0; k < 3; ++k) put<int32_t>(h, 52 + 4 * k, df.pos[k]);
   put<uint64_t>(h, 64, seed);
   put<uint64_t>(h, 72, chain);
-  for (int k = 0; k < 4; ++k) put<uint32_t>(h, 80 + 4 * k, ctr[k]);
+  for (int k = 0; k < 3; ++k) put<uint32_t>(h, 80 + 4 * k, ctr[k]);
+  put<uint32_t>(h, 92, (uint32_t)(open_mu + 1));
   put<double>(h, 96, df.c);
   put<uint64_t>(h, 104, (uint64_t)(n * sizeof(double)));
   put<uint64_t>(h, 112, fnv1a(links.data(), n * sizeof(double)));
@@ -132,6 +136,7 @@ klft_status klft_checkpoint_read(const char *path, klft_lattice **out) {
   long long V = 1;
   for (int d = 0; d < 4; ++d) L[d] = get<int32_t>(h, 24 + 4 * d);
   if (nc < 1 || nc > 3 || nd < 2 || nd > 4) return fail(KLFT_EINVAL, "klft_checkpoint_read: bad group or dims");
+  if (get<uint32_t>(h, 92) > (uint32_t)nd) return fail(KLFT_EINVAL, "klft_checkpoint_read: bad open-boundary direction");
   for (int d = 0; d < nd; ++d) {
     if (L[d] < 2 || (L[d] & 1)) return fail(KLFT_EINVAL, "klft_checkpoint_read: bad extent");
     V *= L[d];
@@ -153,9 +158,11 @@ klft_status klft_checkpoint_read(const char *path, klft_lattice **out) {
     const int pos[3] = {get<int32_t>(h, 52), get<int32_t>(h, 56), get<int32_t>(h, 60)};
     s = klft_lattice_set_defect(lat, get<int32_t>(h, 48), pos, get<double>(h, 96));
   }
+  const uint32_t open1 = get<uint32_t>(h, 92);
+  if (s == KLFT_OK && open1 > 0) s = klft_lattice_set_open_boundary(lat, (int)open1 - 1);
   if (s == KLFT_OK) {
-    uint32_t ctr[4];
-    for (int k = 0; k < 4; ++k) ctr[k] = get<uint32_t>(h, 80 + 4 * k);
+    uint32_t ctr[4] = {0, 0, 0, 0};
+    for (int k = 0; k < 3; ++k) ctr[k] = get<uint32_t>(h, 80 + 4 * k);
     std::lock_guard<std::mutex> g(lat->mtx);
     cudaError_t e = cudaMemcpyAsync(lat->d_counters, ctr, sizeof ctr, cudaMemcpyHostToDevice, lat->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(lat->stream);

@@ -257,6 +257,7 @@ struct Geom {
   int H[4];      // half extents
   int hs[4];     // hidx strides
   long long V, Vh;
+  int open_mu;  // open boundary: links U_open_mu on the slice x_open_mu = L - 1 are zero (-1: periodic)
   // select-based access for directions known only at run time, so that a kernel
   // parameter Geom is read from the constant bank instead of a local copy
   KLFT_HD int Ld(int d) const { return d == 0 ? L[0] : (d == 1 ? L[1] : (d == 2 ? L[2] : L[3])); }
@@ -293,6 +294,10 @@ KLFT_HD long long site_lin(const Geom &g, const Site &s) {
     hidx += (long long)s.h(d) * g.hs[d];
   }
   return (long long)sub * g.Vh + hidx;
+}
+// a link across the open boundary (zero, never updated)
+KLFT_HD bool open_link(const Geom &g, const Site &s, int mu) {
+  return mu == g.open_mu && 2 * s.h(mu) + s.b(mu) == g.Ld(mu) - 1;
 }
 // lexicographic site index, x0 fastest (random-stream key and host layout)
 KLFT_HD uint32_t site_lex(const Geom &g, const Site &s) {

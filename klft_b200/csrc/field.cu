@@ -63,6 +63,7 @@ __global__ void reunitarize_kernel(Links<NC, T> U, Geom g) {
   if (t >= g.V * g.nd) return;
   const int mu = (int)(t / g.V);
   const long long lin = t - (long long)mu * g.V;
+  if (g.open_mu == mu && open_link(g, site_from_lin(g, lin), mu)) return;
   const Mat<NC, T> m = U.load(lin, mu);
   Mat<NC, double> d;
 #pragma unroll
@@ -78,6 +79,15 @@ __global__ void reunitarize_kernel(Links<NC, T> U, Geom g) {
   U.store(lin, mu, o);
 }
 
+// open boundary in direction g.open_mu: zero the links on the last slice
+template <int NC, typename T>
+__global__ void open_boundary_kernel(Links<NC, T> U, Geom g) {
+  const long long lin = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (lin >= g.V) return;
+  if (!open_link(g, site_from_lin(g, lin), g.open_mu)) return;
+  U.store(lin, g.open_mu, mzero<NC, T>());
+}
+
 template <int NC, typename T>
 __global__ void unitarity_kernel(Links<NC, T> U, Geom g, double *part) {
   double worst = 0.0;
@@ -85,6 +95,7 @@ __global__ void unitarity_kernel(Links<NC, T> U, Geom g, double *part) {
        t += (long long)gridDim.x * blockDim.x) {
     const int mu = (int)(t / g.V);
     const long long lin = t - (long long)mu * g.V;
+    if (g.open_mu == mu && open_link(g, site_from_lin(g, lin), mu)) continue;
     const Mat<NC, T> m = U.load(lin, mu);
     Mat<NC, double> d;
 #pragma unroll
@@ -183,6 +194,13 @@ cudaError_t launch_export(int nc, int dtype, const void *links, const Geom &g, d
 
 cudaError_t launch_reunitarize(int nc, int dtype, void *links, const Geom &g, cudaStream_t st) {
   KLFT_DISPATCH_NC_T(nc, dtype, (reunitarize_kernel<NC, T><<<nblocks(g.V * g.nd, 256), 256, 0, st>>>(
+                                    Links<NC, T>{(cx<T> *)links, g.V}, g)));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_open_boundary(int nc, int dtype, void *links, const Geom &g, cudaStream_t st) {
+  if (g.open_mu < 0) return cudaSuccess;
+  KLFT_DISPATCH_NC_T(nc, dtype, (open_boundary_kernel<NC, T><<<nblocks(g.V, 256), 256, 0, st>>>(
                                     Links<NC, T>{(cx<T> *)links, g.V}, g)));
   return cudaGetLastError();
 }

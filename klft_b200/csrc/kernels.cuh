@@ -23,6 +23,8 @@ cudaError_t launch_init(int nc, int dtype, void *links, const Geom &g, int hot, 
 // host AoS FP64 staging buffer <-> device layout
 cudaError_t launch_import(int nc, int dtype, void *links, const Geom &g, const double *aos, cudaStream_t st);
 cudaError_t launch_export(int nc, int dtype, const void *links, const Geom &g, double *aos, cudaStream_t st);
+// zero the links across the open boundary (no-op when periodic)
+cudaError_t launch_open_boundary(int nc, int dtype, void *links, const Geom &g, cudaStream_t st);
 cudaError_t launch_reunitarize(int nc, int dtype, void *links, const Geom &g, cudaStream_t st);
 // max ||U^dagger U - 1||_F -> *d_out (via partials)
 cudaError_t launch_unitarity(int nc, int dtype, const void *links, const Geom &g, double *d_part, double *d_out,

@@ -124,6 +124,7 @@ KLFT_D int site_update_ref(const Links<NC, T> &U, const Geom &g, const Site &x, 
   const T bnc = (T)a.beta / (T)NC;
 #pragma unroll 1
   for (int mu = 0; mu < ND; ++mu) {
+    if (open_link(g, x, mu)) continue;
     const Mat<NC, T> S = staple<NC, ND, T, DF>(U, g, x, mu, df);
     const bool dlink = DF && df.active && in_defect(g, df, x, mu);
     Mat<NC, T> Uo = U.load(lx, mu);
@@ -168,6 +169,7 @@ KLFT_D int site_update_exp(const Links<3, T> &U, const Geom &g, const Site &x, c
   const T half_eps = (T)(0.5 * a.eps);
 #pragma unroll 1
   for (int mu = 0; mu < ND; ++mu) {
+    if (open_link(g, x, mu)) continue;
     const uint32_t h0 = (uint32_t)(mu * a.nhits);
     Mat<3, T> M;
     {

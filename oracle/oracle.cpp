@@ -321,6 +321,10 @@ static inline void randsun(Mat<3> &r, Stream &g, double delta, int, double) {
 }
 
 // ---------------------------------------------------------------- geometry
+// Open boundary (the intent of GaugeField.hpp:168-185 openBC<mu>): links
+// U_mu on the slice x_mu = L_mu - 1 are zero and never updated.  -1: periodic.
+static int g_open_mu = -1;
+
 struct Geo {
   int nd;
   int L[4];
@@ -333,6 +337,12 @@ struct Geo {
     long s = 0;
     for (int d = nd - 1; d >= 0; --d) s = s * L[d] + x[d];
     return s;
+  }
+  bool open_link(long s, int mu) const {
+    if (mu != g_open_mu) return false;
+    int x[4];
+    coords(s, x);
+    return x[mu] == L[mu] - 1;
   }
   void coords(long s, int x[4]) const {
     for (int d = 0; d < 4; ++d) x[d] = 0;
@@ -475,6 +485,7 @@ static double metropolis_sweep(const Field<NC> &F, double beta, double delta, in
       const ExpHit eh(seed, chain, (uint32_t)s, sweep);
       const bool expprop = NC == 3 && proposal == PROPOSAL_EXP;
       for (int mu = 0; mu < nd; ++mu) {
+        if (g.open_link(s, mu)) continue;
         const Mat<NC> S = staple(F, s, mu);
         const double c = link_factor(g, F.df, s, mu);
         // exp(i eps H) proposals: accepted products U r are kept unprojected
@@ -695,7 +706,8 @@ static void integrate(const Field<NC> &F, double *P, double beta, double tau, in
     }
   }
   for (long s = 0; s < F.g.V; ++s)
-    for (int mu = 0; mu < F.g.nd; ++mu) F.put(s, mu, restore(F.raw(s, mu)));
+    for (int mu = 0; mu < F.g.nd; ++mu)
+      if (!F.g.open_link(s, mu)) F.put(s, mu, restore(F.raw(s, mu)));
 }
 
 // HMC.hpp:48-71: refresh P, H_old, integrate, H_new, accept/reject
@@ -787,6 +799,8 @@ int oracle_uniforms(uint64_t seed, uint64_t chain, uint32_t site, uint32_t step,
   for (int i = 0; i < n; ++i) out[i] = st.next();
   return 0;
 }
+
+void oracle_set_open_boundary(int mu) { g_open_mu = mu; }
 
 int oracle_init(int nc, int nd, const int *L, int hot, uint64_t seed, uint64_t chain, double *U) {
   Geo g(nd, L);

@@ -85,6 +85,8 @@ class Oracle:
                                         C.c_double, C.c_uint64, C.c_uint64, C.c_uint32, C.c_int, _ip, C.c_double,
                                         _dp]
         L.oracle_expi_su3.argtypes = [_dp, _dp]
+        L.oracle_set_open_boundary.argtypes = [C.c_int]
+        L.oracle_set_open_boundary.restype = None
         L.oracle_gauge_force.argtypes = [C.c_int, C.c_int, _ip, _dp, C.c_double, _dp]
         L.oracle_momenta.argtypes = [C.c_int, C.c_int, _ip, C.c_uint64, C.c_uint64, C.c_uint32, _dp]
         L.oracle_gauge_action.argtypes = [C.c_int, C.c_int, _ip, _dp, C.c_double, _dp]
@@ -145,6 +147,10 @@ class Oracle:
         o = np.zeros(len(p))
         self.lib.oracle_wilson_temporal(lat.nc, lat.nd, _i(lat.Lc), _d(U), _i(p), len(p), _d(o))
         return o
+
+    def set_open_boundary(self, mu: int) -> None:
+        """Open boundary in direction mu for the following calls (-1: periodic)."""
+        self.lib.oracle_set_open_boundary(mu)
 
     def metropolis(self, lat: Lat, U, beta, delta, nhits, nsweeps, seed, chain=0, sweep0=0,
                    proposal=PROPOSAL_REFERENCE, eps=0.0, defect=None, defect_c=1.0):

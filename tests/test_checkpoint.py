@@ -14,7 +14,7 @@ def sample(nc=2, L=(4, 4, 2, 2), prec=1):
     rng = np.random.default_rng(3)
     V = int(np.prod(L))
     links = rng.normal(size=(V, len(L), nc, nc)) + 1j * rng.normal(size=(V, len(L), nc, nc))
-    return cio.Checkpoint(nc=nc, L=list(L), precision=prec, seed=11, chain=4, counters=(7, 2, 1, 0),
+    return cio.Checkpoint(nc=nc, L=list(L), precision=prec, seed=11, chain=4, counters=(7, 2, 1), open_mu=2,
                           defect_len=2, defect_pos=(1, 0, 1), defect_c=0.25, links=links)
 
 
@@ -28,6 +28,7 @@ def test_roundtrip_of_the_python_writer(tmp_path):
     assert (back.nc, back.L, back.precision, back.seed, back.chain, back.counters) == \
         (ck.nc, ck.L, ck.precision, ck.seed, ck.chain, ck.counters)
     assert (back.defect_len, back.defect_pos, back.defect_c) == (2, (1, 0, 1), 0.25)
+    assert back.open_mu == 2
 
 
 def corrupt(data: bytes, off: int) -> bytes:

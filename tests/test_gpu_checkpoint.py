@@ -55,7 +55,7 @@ def test_hmc_resume_is_exact(tmp_path):
 def test_host_written_checkpoint_loads(tmp_path):
     g = GaugeField((4, 4, 4, 4), 3, "fp64", "hot", 21)
     U = g.download()
-    ck = cio.Checkpoint(nc=3, L=[4, 4, 4, 4], precision=0, seed=21, chain=0, counters=(5, 0, 0, 0), links=U)
+    ck = cio.Checkpoint(nc=3, L=[4, 4, 4, 4], precision=0, seed=21, chain=0, counters=(5, 0, 0), links=U)
     p = str(tmp_path / "host.ckpt")
     cio.write(p, ck)
     r = GaugeField.load(p)

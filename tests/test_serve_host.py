@@ -36,7 +36,7 @@ def test_poisson_stream_is_seeded_and_in_range():
 
 def test_footprint_counts_what_a_job_holds():
     m = JobSpec(kind="metropolis", nc=3, extents=(16, 16, 16, 16), precision="mixed", plaquette=True)
-    links = 16 ** 4 * 4 * 9 * 8
+    links = 16 ** 4 * 4 * 6 * 8  # mixed-form SU(3) links keep two rows (12 reals)
     fm = footprint(m)
     assert links < fm < links + (1 << 20)
     h = JobSpec(kind="hmc", nc=3, extents=(16, 16, 16, 16), precision="mixed", ntraj=10)
@@ -45,7 +45,7 @@ def test_footprint_counts_what_a_job_holds():
     w = JobSpec(kind="metropolis", nc=3, extents=(16, 16, 16, 16), precision="mixed", wilson_pairs=[(2, 2)])
     assert footprint(w) > fm
     d = JobSpec(kind="metropolis", nc=3, extents=(16, 16, 16, 16), precision="fp64")
-    assert footprint(d) > 2 * links
+    assert footprint(d) > 16 ** 4 * 4 * 9 * 16
 
 
 @pytest.mark.parametrize("bad", [
