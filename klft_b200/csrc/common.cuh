@@ -359,12 +359,17 @@ KLFT_HD Site site_from_lex(const Geom &g, long long lex) {
 }
 
 // ------------------------------------------------------------------ link field view
-// Stored colour planes per link: all N*N, except SU(3) in the mixed (FP32)
-// form, which keeps rows 0 and 1 (12 reals) and rebuilds row 2 as
-// conj(row0 x row1), the unit-determinant completion of two orthonormal rows.
+// Stored colour planes per link: all N*N, except in the mixed (FP32) form
+// SU(3), which keeps rows 0 and 1 (12 reals) and rebuilds row 2 as
+// conj(row0 x row1), the unit-determinant completion of two orthonormal rows,
+// and SU(2), which keeps row 0 (a, b) (4 reals) and rebuilds row 1 as
+// (-conj(b), conj(a)).
 template <int N, typename T> struct LinkPlanes { static constexpr int n = N * N; };
 template <> struct LinkPlanes<3, float> { static constexpr int n = 6; };
-KLFT_HD int link_planes(int nc, int dtype) { return (nc == 3 && dtype == 1) ? 6 : nc * nc; }
+template <> struct LinkPlanes<2, float> { static constexpr int n = 2; };
+KLFT_HD int link_planes(int nc, int dtype) {
+  return dtype == 1 && nc == 3 ? 6 : (dtype == 1 && nc == 2 ? 2 : nc * nc);
+}
 
 template <int N, typename T> struct Links {
   cx<T> *p;
@@ -378,7 +383,7 @@ template <int N, typename T> struct Links {
       for (int i = 0; i < N; ++i)
 #pragma unroll
         for (int j = 0; j < N; ++j) m.e[i][j] = q[(i * N + j) * V];
-    } else {
+    } else if constexpr (N == 3) {
 #pragma unroll
       for (int i = 0; i < 2; ++i)
 #pragma unroll
@@ -386,6 +391,11 @@ template <int N, typename T> struct Links {
       m.e[2][0] = conj(m.e[0][1] * m.e[1][2] - m.e[0][2] * m.e[1][1]);
       m.e[2][1] = conj(m.e[0][2] * m.e[1][0] - m.e[0][0] * m.e[1][2]);
       m.e[2][2] = conj(m.e[0][0] * m.e[1][1] - m.e[0][1] * m.e[1][0]);
+    } else {
+      m.e[0][0] = q[0];
+      m.e[0][1] = q[V];
+      m.e[1][0] = mk<T>(-m.e[0][1].re, m.e[0][1].im);
+      m.e[1][1] = conj(m.e[0][0]);
     }
     return m;
   }
