@@ -37,17 +37,58 @@ klft_status cuda_fail(cudaError_t e, const char *what) {
 
 cudaError_t Scratch::ensure(size_t bytes) {
   if (bytes <= cap) return cudaSuccess;
-  if (ptr) cudaFree(ptr);
-  ptr = nullptr;
-  cap = 0;
-  cudaError_t e = cudaMalloc(&ptr, bytes);
+  release();
+  cudaError_t e = stream ? cudaMallocAsync(&ptr, bytes, stream) : cudaMalloc(&ptr, bytes);
   if (e == cudaSuccess) cap = bytes;
+  else ptr = nullptr;
   return e;
 }
 void Scratch::release() {
-  if (ptr) cudaFree(ptr);
+  if (ptr) {
+    if (stream) cudaFreeAsync(ptr, stream);
+    else cudaFree(ptr);
+  }
   ptr = nullptr;
   cap = 0;
+}
+
+namespace {
+std::mutex g_pin_mu;
+std::vector<double *> g_pin_free;
+std::mutex g_pool_mu;
+std::vector<int> g_pool_done;
+}  // namespace
+
+double *pinned_slots_get() {
+  {
+    std::lock_guard<std::mutex> g(g_pin_mu);
+    if (!g_pin_free.empty()) {
+      double *p = g_pin_free.back();
+      g_pin_free.pop_back();
+      return p;
+    }
+  }
+  double *p = nullptr;
+  if (cudaMallocHost(&p, KLFT_RESULT_SLOTS * sizeof(double)) != cudaSuccess) return nullptr;
+  return p;
+}
+
+void pinned_slots_put(double *p) {
+  if (!p) return;
+  std::lock_guard<std::mutex> g(g_pin_mu);
+  g_pin_free.push_back(p);
+}
+
+void keep_pool_memory(int device) {
+  std::lock_guard<std::mutex> g(g_pool_mu);
+  for (int d : g_pool_done)
+    if (d == device) return;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    uint64_t keep = ~0ull;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  g_pool_done.push_back(device);
 }
 
 }  // namespace klft
@@ -148,15 +189,23 @@ klft_status klft_lattice_create(int nc, int ndims, const int *L, int precision, 
   lat->link_bytes = (size_t)V * ndims * link_planes(nc, lat->dtype()) * elem_bytes(precision);
   e = cudaStreamCreateWithFlags(&lat->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) { delete lat; return cuda_fail(e, "cudaStreamCreate"); }
-  e = cudaMalloc(&lat->links, lat->link_bytes);
+  keep_pool_memory(lat->device);
+  for (Scratch *sc : {&lat->s_part, &lat->s_out, &lat->s_aux, &lat->s_stage, &lat->s_wl, &lat->s_hmc, &lat->s_gf,
+                      &lat->s_tab, &lat->s_tune})
+    sc->stream = lat->stream;
+  e = cudaMallocAsync(&lat->links, lat->link_bytes, lat->stream);
   if (e != cudaSuccess) {
-    cudaStreamDestroy(lat->stream);
-    delete lat;
-    return cuda_fail(e, "cudaMalloc(links)");
+    lat->links = nullptr;
+    klft_status st = cuda_fail(e, "cudaMallocAsync(links)");
+    klft_lattice_destroy(lat);
+    return st;
   }
-  e = cudaMalloc(&lat->d_counters, 4 * sizeof(uint32_t));
+  e = cudaMallocAsync(&lat->d_counters, 4 * sizeof(uint32_t), lat->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(lat->d_counters, 0, 4 * sizeof(uint32_t), lat->stream);
-  if (e == cudaSuccess) e = cudaMallocHost(&lat->h_results, KLFT_RESULT_SLOTS * sizeof(double));
+  if (e == cudaSuccess) {
+    lat->h_results = pinned_slots_get();
+    if (!lat->h_results) e = cudaErrorMemoryAllocation;
+  }
   if (e == cudaSuccess)
     e = launch_init(nc, precision == KLFT_PRECISION_FP64 ? 0 : 1, lat->links, g, start == KLFT_START_HOT, seed, 0,
                     lat->stream);
@@ -178,9 +227,10 @@ klft_status klft_lattice_destroy(klft_lattice *lat) {
     for (Scratch *s : {&lat->s_part, &lat->s_out, &lat->s_aux, &lat->s_stage, &lat->s_wl, &lat->s_hmc,
                         &lat->s_gf, &lat->s_tab, &lat->s_tune})
       s->release();
-    if (lat->links) cudaFree(lat->links);
-    if (lat->d_counters) cudaFree(lat->d_counters);
-    if (lat->h_results) cudaFreeHost(lat->h_results);
+    // stream-ordered frees: no device-wide synchronisation
+    if (lat->links) cudaFreeAsync(lat->links, lat->stream);
+    if (lat->d_counters) cudaFreeAsync(lat->d_counters, lat->stream);
+    pinned_slots_put(lat->h_results);
     if (lat->stream) cudaStreamDestroy(lat->stream);
   }
   delete lat;

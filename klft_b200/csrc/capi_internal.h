@@ -14,13 +14,23 @@
 
 namespace klft {
 
-// A growable device buffer owned by a handle.
+// A growable device buffer owned by a handle.  With a stream attached it is
+// allocated and freed stream-ordered on that stream (cudaMallocAsync /
+// cudaFreeAsync), which never synchronises the device.
 struct Scratch {
   void *ptr = nullptr;
   size_t cap = 0;
+  cudaStream_t stream = nullptr;
   cudaError_t ensure(size_t bytes);
   void release();
 };
+
+// Pinned host result slots (KLFT_RESULT_SLOTS doubles), reused across lattices:
+// cudaFreeHost would synchronise the device whenever a lattice is destroyed.
+double *pinned_slots_get();
+void pinned_slots_put(double *p);
+// The device's default memory pool keeps freed memory for reuse (once per device).
+void keep_pool_memory(int device);
 
 klft_status fail(klft_status code, const char *fmt, ...);
 klft_status cuda_fail(cudaError_t e, const char *what);
