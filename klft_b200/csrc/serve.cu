@@ -11,8 +11,11 @@
 //   * Metropolis rounds: every running Metropolis job gets one sweep per round
 //     step, all jobs of a step in multi-chain launches (one per parity class
 //     and lattice group, enqueue_multi_sweep), then one counter-advance
-//     launch.  kRoundsInFlight rounds are queued ahead on the server stream, so
-//     a job that arrives while a round runs joins the next one.
+//     launch.  Jobs are split into kClasses size classes by the cost of a sweep,
+//     each with its own round pipeline on its own stream, so small (latency-
+//     bound) lattices do not wait for the sweeps of large ones and run beside
+//     them.  kRoundsInFlight rounds are queued ahead per class, so a job that
+//     arrives while a round runs joins its class's next round.
 //   * HMC jobs run trajectory by trajectory on their lattice's own stream, at
 //     most kTrajAhead trajectories ahead, overlapping the rounds.
 //   * a finished job is measured on its own stream (after the round holding its
@@ -51,6 +54,7 @@ namespace {
 constexpr int kSweepsPerRound = 4;  // round steps (sweeps per running job) per round
 constexpr int kRoundsInFlight = 2;
 constexpr int kTrajAhead = 2;
+constexpr int kClasses = 3;  // Metropolis size classes (separate round streams)
 // result slots in lat->s_out / lat->h_results
 constexpr int kSlotPlaq = 0, kSlotHmc = 4, kSlotWilson = 8;  // wilson: kSlotWilson + mu * KLFT_JOB_MAX_WILSON + k
 constexpr int kSlotsUsed = kSlotWilson + 3 * KLFT_JOB_MAX_WILSON;
@@ -67,6 +71,7 @@ struct Job {
   // worker-owned from admission on
   klft_lattice *lat = nullptr;
   int slot = -1;  // accept-counter index (Metropolis)
+  int cls = 0;    // Metropolis size class
   int todo = 0;   // sweeps or trajectories not yet enqueued
   int issued = 0, done_traj = 0;
   bool finishing = false, canceled = false;
@@ -97,6 +102,15 @@ unsigned long long job_link_updates(const klft_job &d) {
 }
 
 bool finite(double x) { return std::isfinite(x); }
+
+// Metropolis size class by the cost of one sweep: links x a per-group weight
+// (U(1) 1, SU(2) 3, SU(3) 10), doubled for FP64.  Class 0 holds lattices whose
+// sweeps are launch- and latency-bound, class 2 the ones that fill the GPU.
+int size_class(const klft_job &d) {
+  const double w = d.nc == 1 ? 1.0 : (d.nc == 2 ? 3.0 : 10.0);
+  const double c = (double)job_volume(d) * d.ndims * w * (d.precision == KLFT_PRECISION_FP64 ? 2.0 : 1.0);
+  return c < 1.0e6 ? 0 : (c < 8.0e6 ? 1 : 2);
+}
 
 klft_status validate(const klft_job *j) {
   if (!j) return fail(KLFT_EINVAL, "klft_server_submit: null job");
@@ -175,12 +189,13 @@ struct klft_server {
 
   // worker-owned
   std::thread worker;
-  cudaStream_t stream = nullptr;
+  cudaStream_t stream = nullptr;  // class 0 (and server-level work)
+  cudaStream_t cls_stream[kClasses] = {};
   unsigned long long *d_nacc = nullptr, *h_nacc = nullptr;
   uint32_t *d_zero = nullptr;
   std::vector<int> free_slots;
   std::vector<std::unique_ptr<Job>> jobs;  // running (admitted) jobs
-  std::deque<cudaEvent_t> rounds;          // in flight, oldest first
+  std::deque<cudaEvent_t> rounds[kClasses];  // in flight per class, oldest first
   std::vector<cudaEvent_t> event_pool;
   double busy_since = -1.0;
 
@@ -200,7 +215,7 @@ struct klft_server {
   void admit(std::unique_ptr<Job> j);
   void finish(Job &j, bool failed, int status, const char *msg);
   void fail_all(const char *msg);
-  bool enqueue_round();
+  bool enqueue_round(int cls);
   void start_measure(Job &j, cudaEvent_t after);
   cudaEvent_t get_event() {
     if (!event_pool.empty()) {
@@ -280,11 +295,12 @@ void klft_server::admit(std::unique_ptr<Job> jp) {
     else {
       j.slot = free_slots.back();
       free_slots.pop_back();
-      ck(cudaMemsetAsync(d_nacc + j.slot, 0, sizeof(unsigned long long), stream), "clear accept counter");
+      j.cls = size_class(j.d);
+      ck(cudaMemsetAsync(d_nacc + j.slot, 0, sizeof(unsigned long long), cls_stream[j.cls]), "clear accept counter");
     }
     j.todo = j.d.nsweeps;
   }
-  // the lattice was initialised on its own stream: later rounds on the server
+  // the lattice was initialised on its own stream: later rounds on the class
   // stream must see it
   if (s == KLFT_OK) ck(cudaStreamSynchronize(lat->stream), "admission");
   if (s != KLFT_OK) return bail(s);
@@ -372,10 +388,12 @@ void klft_server::finish(Job &j, bool failed, int status, const char *msg) {
 
 // One round: kSweepsPerRound steps; step k sweeps every Metropolis job with
 // more than k sweeps left.  Returns false when no job needed a sweep.
-bool klft_server::enqueue_round() {
+bool klft_server::enqueue_round(int cls) {
+  cudaStream_t stream = cls_stream[cls];
   std::vector<Job *> metro;
   for (auto &jp : jobs)
-    if (jp->d.kind == KLFT_JOB_METROPOLIS && !jp->finishing && jp->todo > 0) metro.push_back(jp.get());
+    if (jp->d.kind == KLFT_JOB_METROPOLIS && jp->cls == cls && !jp->finishing && jp->todo > 0)
+      metro.push_back(jp.get());
   if (metro.empty()) return false;
   for (int k = 0; k < kSweepsPerRound; ++k) {
     std::vector<SweepItem> items;
@@ -398,7 +416,7 @@ bool klft_server::enqueue_round() {
   }
   cudaEvent_t ev = get_event();
   if (cudaEventRecord(ev, stream) != cudaSuccess) throw std::runtime_error("cudaEventRecord(round)");
-  rounds.push_back(ev);
+  rounds[cls].push_back(ev);
   nrounds++;
   for (Job *j : metro) {
     j->todo -= std::min(j->todo, kSweepsPerRound);
@@ -430,11 +448,12 @@ bool klft_server::step() {
     progress = true;
   }
   // 2. retire completed rounds
-  while (!rounds.empty() && cudaEventQuery(rounds.front()) == cudaSuccess) {
-    event_pool.push_back(rounds.front());
-    rounds.pop_front();
-    progress = true;
-  }
+  for (auto &rq : rounds)
+    while (!rq.empty() && cudaEventQuery(rq.front()) == cudaSuccess) {
+      event_pool.push_back(rq.front());
+      rq.pop_front();
+      progress = true;
+    }
   // 3. cancellations of running jobs: stop scheduling, wait for their work in flight
   for (auto &jp : jobs) {
     Job &j = *jp;
@@ -467,8 +486,9 @@ bool klft_server::step() {
       progress = true;
     }
   }
-  // 5. Metropolis rounds on the server stream
-  while ((int)rounds.size() < kRoundsInFlight && enqueue_round()) progress = true;
+  // 5. Metropolis rounds, one pipeline per size class
+  for (int k = 0; k < kClasses; ++k)
+    while ((int)rounds[k].size() < kRoundsInFlight && enqueue_round(k)) progress = true;
   // 6. completions
   for (size_t i = 0; i < jobs.size();) {
     Job &j = *jobs[i];
@@ -492,14 +512,16 @@ bool klft_server::step() {
 
 // After an exception: wait for the device work of every running job, then fail them.
 void klft_server::fail_all(const char *msg) {
-  cudaStreamSynchronize(stream);
+  for (cudaStream_t cs : cls_stream) cudaStreamSynchronize(cs);
   for (auto &jp : jobs) {
     if (jp->lat) cudaStreamSynchronize(jp->lat->stream);
     finish(*jp, true, KLFT_EINTERNAL, msg);
   }
   jobs.clear();
-  for (cudaEvent_t e : rounds) event_pool.push_back(e);
-  rounds.clear();
+  for (auto &rq : rounds) {
+    for (cudaEvent_t e : rq) event_pool.push_back(e);
+    rq.clear();
+  }
   cudaGetLastError();
 }
 
@@ -525,7 +547,7 @@ void klft_server::run() {
     }
   }
   // shutdown: wait for work in flight, free everything; queued jobs are dropped
-  cudaStreamSynchronize(stream);
+  for (cudaStream_t cs : cls_stream) cudaStreamSynchronize(cs);
   for (auto &jp : jobs) {
     if (jp->lat) cudaStreamSynchronize(jp->lat->stream);
     release_job(*this, *jp);
@@ -569,6 +591,9 @@ klft_status klft_server_create(int device, uint64_t budget_bytes, int max_active
   s->budget = budget_bytes;
   s->st.bytes_budget = budget_bytes;
   e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+  s->cls_stream[0] = s->stream;
+  for (int k = 1; k < kClasses && e == cudaSuccess; ++k)
+    e = cudaStreamCreateWithFlags(&s->cls_stream[k], cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaMalloc(&s->d_nacc, (size_t)s->max_active * sizeof(unsigned long long));
   if (e == cudaSuccess) e = cudaMallocHost(&s->h_nacc, (size_t)s->max_active * sizeof(unsigned long long));
   if (e == cudaSuccess) e = cudaMalloc(&s->d_zero, 16);
@@ -578,6 +603,8 @@ klft_status klft_server_create(int device, uint64_t budget_bytes, int max_active
     if (s->d_nacc) cudaFree(s->d_nacc);
     if (s->h_nacc) cudaFreeHost(s->h_nacc);
     if (s->d_zero) cudaFree(s->d_zero);
+    for (int k = 1; k < kClasses; ++k)
+      if (s->cls_stream[k]) cudaStreamDestroy(s->cls_stream[k]);
     if (s->stream) cudaStreamDestroy(s->stream);
     cudaSetDevice(prev);
     return st;
@@ -602,11 +629,14 @@ klft_status klft_server_destroy(klft_server *s) {
   int prev = 0;
   cudaGetDevice(&prev);
   cudaSetDevice(s->device);
-  for (cudaEvent_t e : s->rounds) cudaEventDestroy(e);
+  for (auto &rq : s->rounds)
+    for (cudaEvent_t e : rq) cudaEventDestroy(e);
   for (cudaEvent_t e : s->event_pool) cudaEventDestroy(e);
   if (s->d_nacc) cudaFree(s->d_nacc);
   if (s->h_nacc) cudaFreeHost(s->h_nacc);
   if (s->d_zero) cudaFree(s->d_zero);
+  for (int k = 1; k < kClasses; ++k)
+    if (s->cls_stream[k]) cudaStreamDestroy(s->cls_stream[k]);
   if (s->stream) cudaStreamDestroy(s->stream);
   cudaSetDevice(prev);
   delete s;
