@@ -85,9 +85,8 @@ class Dist:
 
     def set_device(self):
         if self.world > 1:
-            from klft_b200 import _lib  # noqa: F401
-            import ctypes
-            ctypes.CDLL("libcudart.so.12", mode=ctypes.RTLD_GLOBAL).cudaSetDevice(self.local)
+            import klft_b200
+            klft_b200.set_device(self.local)
 
     def barrier(self):
         if self.pg:

@@ -53,6 +53,10 @@ const char *klft_last_error(void);
 int klft_version(void);
 /* Number of visible CUDA devices. */
 klft_status klft_device_count(int *n);
+/* Make `device` current for the calling thread; lattices created afterwards on
+ * this thread live there (one process per GPU; the device choice of
+ * Kokkos::initialize in the reference, lib/HMC_SU2.cpp:30). */
+klft_status klft_set_device(int device);
 
 /* Create a gauge field of SU(nc) (nc = 1: U(1)) links on an ndims-dimensional
  * periodic lattice with even extents L[0..ndims-1] on the current device.

@@ -42,6 +42,11 @@ def device_count() -> int:
     return n.value
 
 
+def set_device(device: int) -> None:
+    """Make `device` current for this thread in the library's CUDA runtime."""
+    check(lib().klft_set_device(device))
+
+
 def _pairs(pairs) -> np.ndarray:
     return np.ascontiguousarray(np.array(pairs, dtype=np.int32).reshape(-1, 2))
 

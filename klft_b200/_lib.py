@@ -53,6 +53,7 @@ SIGNATURES = {
     "klft_last_error": (C.c_char_p, []),
     "klft_version": (C.c_int, []),
     "klft_device_count": (C.c_int, [_ip]),
+    "klft_set_device": (C.c_int, [C.c_int]),
     "klft_lattice_create": (C.c_int, [C.c_int, C.c_int, _ip, C.c_int, C.c_int, C.c_uint64, C.POINTER(_vp)]),
     "klft_lattice_destroy": (C.c_int, [_vp]),
     "klft_lattice_info": (C.c_int, [_vp, _ip, _ip, _ip, _ip, _llp]),

@@ -157,6 +157,16 @@ klft_status klft_device_count(int *n) {
   return KLFT_OK;
 }
 
+klft_status klft_set_device(int device) {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) return fail(KLFT_ECUDA, "klft_set_device: no CUDA device available");
+  if (device < 0 || device >= n) return fail(KLFT_EINVAL, "klft_set_device: no device %d (%d present)", device, n);
+  e = cudaSetDevice(device);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+  return KLFT_OK;
+}
+
 klft_status klft_lattice_create(int nc, int ndims, const int *L, int precision, int start, uint64_t seed,
                                 klft_lattice **out) {
   if (!out || !L) return fail(KLFT_EINVAL, "klft_lattice_create: null pointer");
