@@ -466,6 +466,13 @@ klft_status klft_run_cycles(klft_lattice *lat, double beta, double delta, int nh
     const int nblk = plaquette_blocks(lat->g);
     if (lat->s_part.cap < (size_t)nblk * sizeof(double)) CK(lat->s_part.ensure((size_t)nblk * sizeof(double)));
   }
+  // The temporal (1, 1) loop of plane (mu, Nd-1) is that plane's plaquette: when
+  // the pair list holds it, the plaquette kernel covers the spatial planes only
+  // and the temporal planes come from the loop sums (added in FP64 below).
+  int k11 = -1;
+  for (int k = 0; k < npairs && k11 < 0; ++k)
+    if (temporal_pairs[2 * k] == 1 && temporal_pairs[2 * k + 1] == 1) k11 = k;
+  const int plaq_nu_end = k11 >= 0 ? nd - 1 : nd;
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
@@ -476,7 +483,7 @@ klft_status klft_run_cycles(klft_lattice *lat, double beta, double delta, int nh
     if (measure_plaquette) {
       const int nblk = plaquette_blocks(lat->g);
       CK(launch_plaquette(lat->nc, lat->dtype(), lat->links, lat->g, (double *)lat->s_part.ptr, nblk, d_plaq + c,
-                          lat->stream));
+                          lat->stream, plaq_nu_end));
     }
     for (int mu = 0; mu < nd - 1 && npairs > 0; ++mu) {
       // the axial-gauge transformation along nu = Nd-1 is shared by the spatial planes
@@ -502,7 +509,12 @@ klft_status klft_run_cycles(klft_lattice *lat, double beta, double delta, int nh
   norm *= (double)nhits;
   for (int c = 0; c < ncycles; ++c) {
     if (acc_out) acc_out[c] = nhits > 0 ? (double)h_nacc[c] / norm : 0.0;
-    if (plaq_out && measure_plaquette) plaq_out[c] = normalize_plaquette(lat, h_out[c]);
+    if (plaq_out && measure_plaquette) {
+      double sum = h_out[c];
+      if (k11 >= 0)
+        for (int mu = 0; mu < nd - 1; ++mu) sum += h_out[ncycles + (size_t)c * nw + (size_t)mu * npairs + k11];
+      plaq_out[c] = normalize_plaquette(lat, sum);
+    }
     if (w_out)
       for (int k = 0; k < npairs; ++k) {
         double acc = 0.0;

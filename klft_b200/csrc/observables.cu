@@ -57,8 +57,10 @@ KLFT_HD long long window_threads(const Geom &g) { return (long long)(1 << g.nd) 
 template <typename T> struct PlaqMinBlocks { static constexpr int v = 2; };
 template <> struct PlaqMinBlocks<double> { static constexpr int v = 1; };
 
+// planes (mu, nu) with mu < nu < nu_end (nu_end = Nd: all planes)
 template <int NC, int ND, typename T>
-__global__ void __launch_bounds__(RED_THREADS, PlaqMinBlocks<T>::v) plaquette_kernel(Links<NC, T> U, Geom g, double *part) {
+__global__ void __launch_bounds__(RED_THREADS, PlaqMinBlocks<T>::v) plaquette_kernel(Links<NC, T> U, Geom g,
+                                                                                     double *part, int nu_end) {
   double acc = 0.0;
   const long long nthr = window_threads(g);
   for (long long t = (long long)blockIdx.x * RED_THREADS + threadIdx.x; t < nthr;
@@ -71,7 +73,7 @@ __global__ void __launch_bounds__(RED_THREADS, PlaqMinBlocks<T>::v) plaquette_ke
       const Site xpmu = site_up(g, x, mu);
       const Mat<NC, T> umu = U.load(lin, mu);
 #pragma unroll 1
-      for (int nu = mu + 1; nu < ND; ++nu) {
+      for (int nu = mu + 1; nu < nu_end; ++nu) {
         const Mat<NC, T> lmu = mul(umu, U.load(site_lin(g, xpmu), nu));
         const Mat<NC, T> lnu = mul(U.load(lin, nu), U.load(site_lin(g, site_up(g, x, nu)), mu));
         acc += retr_nd<NC, T, double>(lmu, lnu);
@@ -160,8 +162,10 @@ cudaError_t launch_reduce_partials(const double *d_part, int nblk, int n, double
   } while (0)
 
 cudaError_t launch_plaquette(int nc, int dtype, const void *links, const Geom &g, double *d_part, int nblk,
-                             double *d_out, cudaStream_t st) {
-#define KLFT_PQ(NDV) plaquette_kernel<NC, NDV, T><<<nblk, RED_THREADS, 0, st>>>(Links<NC, T>{(cx<T> *)links, g.V}, g, d_part)
+                             double *d_out, cudaStream_t st, int nu_end) {
+  if (nu_end < 0) nu_end = g.nd;
+#define KLFT_PQ(NDV) \
+  plaquette_kernel<NC, NDV, T><<<nblk, RED_THREADS, 0, st>>>(Links<NC, T>{(cx<T> *)links, g.V}, g, d_part, nu_end)
   KLFT_OBS_DISPATCH(nc, dtype, g.nd, ({
     if (g.nd == 2) KLFT_PQ(2);
     else if (g.nd == 3) KLFT_PQ(3);

@@ -1,0 +1,30 @@
+"""klft_run_cycles (the run_metropolis loop, Metropolis.hpp:204-218) against the
+same steps through the single-call API: sweep, GaugePlaquette, WilsonLoop_temporal.
+With (1, 1) among the temporal pairs the cycle takes the temporal plaquettes from
+those loop sums, so both pair lists are checked."""
+import numpy as np
+import pytest
+
+from klft_b200 import GaugeField
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("L,nc", [([4, 4, 6, 8], 3), ([6, 4, 8], 2), ([8, 6], 1), ([4, 6, 4, 4], 2)])
+@pytest.mark.parametrize("pairs", [[(1, 1), (2, 3), (1, 2)], [(2, 2), (3, 1)]])
+@pytest.mark.parametrize("precision,rtol,atol", [("fp64", 1e-12, 1e-14), ("mixed", 0.0, 2e-6)])
+def test_cycles_match_single_calls(L, nc, pairs, precision, rtol, atol):
+    beta = {1: 1.0, 2: 2.3, 3: 6.0}[nc]
+    prop = "exp" if nc == 3 else "reference"
+    a = GaugeField(L, nc, precision, "hot", 31)
+    b = GaugeField(L, nc, precision, "hot", 31)
+    a.set_stream(31, 4)
+    b.set_stream(31, 4)
+    acc, plaq, w, ms = a.run_cycles(beta, 0.3, 3, 3, prop, 0.3, True, pairs)
+    assert ms > 0
+    for c in range(3):
+        acc1 = b.metropolis(beta, 0.3, 3, 1, prop, 0.3)
+        assert acc[c] == acc1[0]
+        assert plaq[c] == pytest.approx(b.plaquette(), rel=rtol, abs=atol)
+        np.testing.assert_allclose(w[c], b.wilson_loop_temporal(pairs), rtol=rtol, atol=atol)
+    np.testing.assert_array_equal(a.download(), b.download())
