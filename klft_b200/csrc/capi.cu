@@ -390,16 +390,28 @@ klft_status klft_wilson_loop_temporal(klft_lattice *lat, const int *pairs, int n
   if (npairs == 0) return KLFT_OK;
   LOCK(lat);
   const int nd = lat->g.nd;
-  std::vector<double> acc(npairs, 0.0), sums(npairs);
+  // one plan and one axial-gauge transformation along nu = Nd-1 for all spatial
+  // planes; a single copy of the (Nd-1) x npairs sums at the end
+  const size_t nsum = (size_t)(nd - 1) * npairs;
+  CK(lat->s_out.ensure((nsum > KLFT_RESULT_SLOTS ? nsum : KLFT_RESULT_SLOTS) * sizeof(double)));
+  WilsonPlan plan;
+  klft_status s = make_wilson_plan(lat, pairs, npairs, nd - 1, plan);
+  if (s != KLFT_OK) return s;
   for (int mu = 0; mu < nd - 1; ++mu) {
-    klft_status s = wilson_sums(lat, mu, nd - 1, pairs, npairs, sums.data());
+    s = enqueue_wilson_plane(lat, plan, mu, nd - 1, mu > 0, (double *)lat->s_out.ptr + (size_t)mu * npairs);
     if (s != KLFT_OK) return s;
-    for (int k = 0; k < npairs; ++k) {
-      const double w = normalize_wilson(lat, sums[k]);
-      acc[k] = mu == 0 ? w : acc[k] + w;
-    }
   }
-  for (int k = 0; k < npairs; ++k) out[k] = acc[k] / (double)(nd - 1);
+  std::vector<double> sums(nsum);
+  CK(cudaMemcpyAsync(sums.data(), lat->s_out.ptr, nsum * sizeof(double), cudaMemcpyDeviceToHost, lat->stream));
+  CK(cudaStreamSynchronize(lat->stream));
+  for (int k = 0; k < npairs; ++k) {
+    double acc = 0.0;
+    for (int mu = 0; mu < nd - 1; ++mu) {
+      const double w = normalize_wilson(lat, sums[(size_t)mu * npairs + k]);
+      acc = mu == 0 ? w : acc + w;
+    }
+    out[k] = acc / (double)(nd - 1);
+  }
   return KLFT_OK;
 }
 
