@@ -23,6 +23,7 @@
 #include "capi_internal.h"
 #include "kernels.cuh"
 #include "metropolis_site.cuh"
+#include "observables.cuh"
 
 namespace klft {
 
@@ -97,8 +98,124 @@ __global__ void copy_labels_kernel(const int *labels, int n, int *dst, const uin
   if (i < n) dst[(size_t)(*slot) * n + i] = labels[i];
 }
 
-__global__ void copy_slot_kernel(const double *src, double *dst, const uint32_t *slot, int stride, int index) {
-  dst[(size_t)(*slot) * stride + index] = *src;
+// Plaquette sums of up to BATCH_MAX lattices of one (Nc, Nd, precision) in one
+// launch: chain k owns CTAs [block_begin, block_begin + nblk) and partials
+// [part_begin, part_begin + nblk).  Each CTA computes exactly the partial that
+// block (blockIdx.x - block_begin) of the single-lattice plaquette launch writes
+// and multi_reduce_kernel sums them in the single-lattice order, so a chain's
+// sum in a batch is bit-identical to its solo plaquette.
+struct PlaqDesc {
+  void *links;
+  Geom g;
+  long long part_begin;
+  int index;  // column of the chain in the result slots
+  int block_begin;
+  int nblk;
+};
+
+struct PlaqTable {
+  int n;
+  PlaqDesc c[BATCH_MAX];
+};
+
+template <int NC, int ND, typename T>
+__global__ void __launch_bounds__(RED_THREADS, PlaqMinBlocks<T>::v)
+    multi_plaquette_kernel(const __grid_constant__ PlaqTable tab, double *__restrict__ part) {
+  int lo = 0, hi = tab.n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (tab.c[mid].block_begin <= (int)blockIdx.x) lo = mid;
+    else hi = mid - 1;
+  }
+  const PlaqDesc &c = tab.c[lo];
+  const int b = (int)blockIdx.x - c.block_begin;
+  const double s = block_sum<RED_THREADS>(
+      plaquette_partial<NC, ND, T>(Links<NC, T>{(cx<T> *)c.links, c.g.V}, c.g, ND, b, c.nblk));
+  if (threadIdx.x == 0) part[c.part_begin + b] = s;
+}
+
+// one CTA per chain of the table: plaq[(*slot) * stride + index] = sum of its partials
+__global__ void multi_reduce_kernel(const __grid_constant__ PlaqTable tab, const double *__restrict__ part,
+                                    double *plaq, const uint32_t *slot, int stride) {
+  const PlaqDesc &c = tab.c[blockIdx.x];
+  double v = 0.0;
+  for (int i = threadIdx.x; i < c.nblk; i += RED_THREADS) v += part[c.part_begin + i];
+  const double s = block_sum<RED_THREADS>(v);
+  if (threadIdx.x == 0) plaq[(size_t)(*slot) * stride + c.index] = s;
+}
+
+template <int NC, typename T>
+cudaError_t launch_multi_plaquette_nc(int nd, const PlaqTable &tab, int blocks, double *part, double *plaq,
+                                      const uint32_t *slot, int stride, cudaStream_t st) {
+  if (nd == 2) multi_plaquette_kernel<NC, 2, T><<<blocks, RED_THREADS, 0, st>>>(tab, part);
+  else if (nd == 3) multi_plaquette_kernel<NC, 3, T><<<blocks, RED_THREADS, 0, st>>>(tab, part);
+  else multi_plaquette_kernel<NC, 4, T><<<blocks, RED_THREADS, 0, st>>>(tab, part);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  multi_reduce_kernel<<<tab.n, RED_THREADS, 0, st>>>(tab, part, plaq, slot, stride);
+  return cudaGetLastError();
+}
+
+// Plaquette sums of all lattices into plaq[(*slot) * stride + index_i], one
+// multi-chain launch pair per (Nc, Nd, precision) group of up to BATCH_MAX;
+// part holds sum_i plaquette_blocks(g_i) doubles.
+cudaError_t enqueue_multi_plaquette(const std::vector<klft_lattice *> &lats, const std::vector<int> &index,
+                                    double *part, double *plaq, const uint32_t *slot, int stride, cudaStream_t st,
+                                    int *nlaunch) {
+  struct Key {
+    int nc, nd, dtype;
+  };
+  std::vector<Key> keys;
+  std::vector<std::vector<int>> members;
+  for (size_t i = 0; i < lats.size(); ++i) {
+    const Key k{lats[i]->nc, lats[i]->g.nd, lats[i]->dtype()};
+    size_t gi = 0;
+    while (gi < keys.size() && !(keys[gi].nc == k.nc && keys[gi].nd == k.nd && keys[gi].dtype == k.dtype)) ++gi;
+    if (gi == keys.size()) {
+      keys.push_back(k);
+      members.emplace_back();
+    }
+    members[gi].push_back((int)i);
+  }
+  long long pbeg = 0;
+  std::unique_ptr<PlaqTable> tab(new PlaqTable());
+  for (size_t gi = 0; gi < keys.size(); ++gi)
+    for (size_t m0 = 0; m0 < members[gi].size(); m0 += BATCH_MAX) {
+      std::memset(tab.get(), 0, sizeof(PlaqTable));
+      int blocks = 0;
+      for (size_t m = m0; m < members[gi].size() && m < m0 + BATCH_MAX; ++m) {
+        const int i = members[gi][m];
+        PlaqDesc &d = tab->c[tab->n++];
+        d.links = lats[i]->links;
+        d.g = lats[i]->g;
+        d.part_begin = pbeg;
+        d.index = index[i];
+        d.block_begin = blocks;
+        d.nblk = plaquette_blocks(d.g);
+        blocks += d.nblk;
+        pbeg += d.nblk;
+      }
+      const Key &k = keys[gi];
+      cudaError_t e;
+      if (k.dtype == 0) {
+        if (k.nc == 1) e = launch_multi_plaquette_nc<1, double>(k.nd, *tab, blocks, part, plaq, slot, stride, st);
+        else if (k.nc == 2) e = launch_multi_plaquette_nc<2, double>(k.nd, *tab, blocks, part, plaq, slot, stride, st);
+        else e = launch_multi_plaquette_nc<3, double>(k.nd, *tab, blocks, part, plaq, slot, stride, st);
+      } else {
+        if (k.nc == 1) e = launch_multi_plaquette_nc<1, float>(k.nd, *tab, blocks, part, plaq, slot, stride, st);
+        else if (k.nc == 2) e = launch_multi_plaquette_nc<2, float>(k.nd, *tab, blocks, part, plaq, slot, stride, st);
+        else e = launch_multi_plaquette_nc<3, float>(k.nd, *tab, blocks, part, plaq, slot, stride, st);
+      }
+      if (e != cudaSuccess) return e;
+      if (nlaunch) *nlaunch += 2;
+    }
+  return cudaSuccess;
+}
+
+long long multi_plaquette_parts(const std::vector<klft_lattice *> &lats) {
+  long long n = 0;
+  for (klft_lattice *l : lats) n += plaquette_blocks(l->g);
+  return n;
 }
 
 // declared in ptbc.cu
@@ -315,15 +432,14 @@ klft_status enqueue_cycle(klft_batch *b, int measure) {
     CK(cudaGetLastError());
   }
   if (measure) {
-    double *plaq = (double *)b->s_plaq.ptr;
+    std::vector<klft_lattice *> lats;
+    std::vector<int> index;
     for (int i = 0; i < n; ++i) {
-      klft_lattice *lat = b->chains[i].lat;
-      const int nblk = plaquette_blocks(lat->g);
-      double *part = (double *)b->s_ppart.ptr;
-      CK(launch_plaquette(lat->nc, lat->dtype(), lat->links, lat->g, part, nblk, part + nblk, b->stream));
-      copy_slot_kernel<<<1, 1, 0, b->stream>>>(part + nblk, plaq, b->d_slot, n, i);
-      CK(cudaGetLastError());
+      lats.push_back(b->chains[i].lat);
+      index.push_back(i);
     }
+    CK(enqueue_multi_plaquette(lats, index, (double *)b->s_ppart.ptr, (double *)b->s_plaq.ptr, b->d_slot, n,
+                               b->stream, nullptr));
   }
   batch_slot_kernel<<<1, 1, 0, b->stream>>>(b->d_slot, b->d_slot + 1);
   CK(cudaGetLastError());
@@ -339,12 +455,9 @@ klft_status prepare(klft_batch *b, int ncycles) {
   CK(b->s_nacc.ensure((size_t)b->cap * n * sizeof(unsigned long long)));
   CK(b->s_plaq.ensure((size_t)b->cap * n * sizeof(double)));
   CK(b->s_labels.ensure((size_t)b->cap * (b->reps.empty() ? 1 : b->reps.size()) * sizeof(int)));
-  int maxblk = 1;
-  for (auto &ch : b->chains) {
-    const int nb = plaquette_blocks(ch.lat->g);
-    maxblk = nb > maxblk ? nb : maxblk;
-  }
-  CK(b->s_ppart.ensure((size_t)(maxblk + 1) * sizeof(double)));
+  std::vector<klft_lattice *> lats;
+  for (auto &ch : b->chains) lats.push_back(ch.lat);
+  CK(b->s_ppart.ensure((size_t)(multi_plaquette_parts(lats) + 1) * sizeof(double)));
   if (!b->d_ctrs) {
     CK(cudaMalloc(&b->d_ctrs, BATCH_MAX * 64 * sizeof(uint32_t *)));
   }
