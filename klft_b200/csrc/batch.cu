@@ -219,9 +219,9 @@ long long multi_plaquette_parts(const std::vector<klft_lattice *> &lats) {
 }
 
 // declared in ptbc.cu
-cudaError_t launch_defect_sums(int nc, int dtype, const void *links, const Geom &g, const Defect &df, double beta,
-                               double *d_part, double *d_out, cudaStream_t st);
-int defect_sums_blocks(const Geom &g);
+cudaError_t enqueue_multi_defect_sums(const std::vector<klft_lattice *> &reps, double beta, double *part, double *A,
+                                      cudaStream_t st);
+long long multi_defect_parts(const std::vector<klft_lattice *> &reps);
 __global__ void ptbc_swap_kernel(int nrep, const double *c_of_label, const double *A, int *label_of_rep,
                                  int *rep_of_label, double *c_of_rep, uint64_t seed, const uint32_t *cycle_ctr,
                                  unsigned long long *swap_acc);
@@ -420,11 +420,9 @@ klft_status enqueue_cycle(klft_batch *b, int measure) {
   CK(launch_advance_many(b->d_ctrs, n, b->stream));
   if (!b->reps.empty()) {
     const int nrep = (int)b->reps.size();
-    for (int r = 0; r < nrep; ++r) {
-      klft_lattice *lat = b->chains[b->reps[r]].lat;
-      CK(launch_defect_sums(lat->nc, lat->dtype(), lat->links, lat->g, lat->defect, b->ptbc_beta, b->d_part,
-                            b->d_A + 2 * r, b->stream));
-    }
+    std::vector<klft_lattice *> reps;
+    for (int r = 0; r < nrep; ++r) reps.push_back(b->chains[b->reps[r]].lat);
+    CK(enqueue_multi_defect_sums(reps, b->ptbc_beta, b->d_part, b->d_A, b->stream));
     ptbc_swap_kernel<<<1, 1, 0, b->stream>>>(nrep, b->d_c_of_label, b->d_A, b->d_label_of_rep, b->d_rep_of_label,
                                              b->d_c_of_rep, b->swap_seed, b->d_slot + 1, b->d_swap_acc);
     CK(cudaGetLastError());
@@ -549,15 +547,12 @@ klft_status klft_batch_set_ptbc(klft_batch *b, const int *chain_ids, int nrep, c
       cudaFree(*p);
       *p = nullptr;
     }
-  int maxblk = 1;
-  for (int r = 0; r < nrep; ++r) {
-    const int nb = defect_sums_blocks(b->chains[chain_ids[r]].lat->g);
-    maxblk = nb > maxblk ? nb : maxblk;
-  }
+  std::vector<klft_lattice *> replats;
+  for (int r = 0; r < nrep; ++r) replats.push_back(b->chains[chain_ids[r]].lat);
   CK(cudaMalloc(&b->d_c_of_label, nrep * sizeof(double)));
   CK(cudaMalloc(&b->d_c_of_rep, nrep * sizeof(double)));
   CK(cudaMalloc(&b->d_A, 2 * nrep * sizeof(double)));
-  CK(cudaMalloc(&b->d_part, 2 * (size_t)maxblk * sizeof(double)));
+  CK(cudaMalloc(&b->d_part, 2 * (size_t)multi_defect_parts(replats) * sizeof(double)));
   CK(cudaMalloc(&b->d_label_of_rep, nrep * sizeof(int)));
   CK(cudaMalloc(&b->d_rep_of_label, nrep * sizeof(int)));
   CK(cudaMalloc(&b->d_swap_acc, nrep * sizeof(unsigned long long)));

@@ -17,16 +17,21 @@
 #include <cmath>
 #include <vector>
 
+#include <cstring>
+#include <vector>
+
 #include "../../include/klft_b200.h"
 #include "capi_internal.h"
 #include "kernels.cuh"
 
 namespace klft {
 
-// A_1, A_2 of one lattice: threads over the sites with x0 = 0 (raw links).
+// Block b's partials of A_1, A_2 of one lattice (256 threads over the sites
+// with x0 = 0, raw links); thread 0 writes out[0], out[1].
 template <int NC, int ND, typename T>
-__global__ void defect_sums_kernel(Links<NC, T> U, Geom g, Defect df, double bnc, double *out) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+KLFT_D void defect_partial(const Links<NC, T> &U, const Geom &g, const Defect &df, double bnc, long long b,
+                           double *out) {
+  long long t = b * 256 + threadIdx.x;
   const long long nsp = g.V / g.L[0];
   double a1 = 0.0, a2 = 0.0;
   if (t < nsp) {
@@ -61,7 +66,7 @@ __global__ void defect_sums_kernel(Links<NC, T> U, Geom g, Defect df, double bnc
   r1[threadIdx.x] = a1;
   r2[threadIdx.x] = a2;
   __syncthreads();
-  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+  for (int s = 128; s > 0; s >>= 1) {
     if ((int)threadIdx.x < s) {
       r1[threadIdx.x] += r1[threadIdx.x + s];
       r2[threadIdx.x] += r2[threadIdx.x + s];
@@ -69,9 +74,63 @@ __global__ void defect_sums_kernel(Links<NC, T> U, Geom g, Defect df, double bnc
     __syncthreads();
   }
   if (threadIdx.x == 0) {
-    out[2 * blockIdx.x] = r1[0];
-    out[2 * blockIdx.x + 1] = r2[0];
+    out[0] = r1[0];
+    out[1] = r2[0];
   }
+}
+
+template <int NC, int ND, typename T>
+__global__ void __launch_bounds__(256) defect_sums_kernel(Links<NC, T> U, Geom g, Defect df, double bnc,
+                                                          double *out) {
+  defect_partial<NC, ND, T>(U, g, df, bnc, blockIdx.x, out + 2 * blockIdx.x);
+}
+
+// A_1, A_2 of up to 64 replicas of one (Nc, Nd, precision) in one launch:
+// replica k owns CTAs [block_begin, block_begin + nblk) and partial pairs
+// [part_begin, part_begin + nblk); multi_defect_reduce_kernel adds them in the
+// single-lattice order into A[2 rep], A[2 rep + 1], so a replica's sums in a
+// batch are bit-identical to klft_ptbc_defect_sums.
+struct DefectDesc {
+  void *links;
+  Geom g;
+  Defect df;
+  int rep;
+  int block_begin;
+  int nblk;
+  int part_begin;
+};
+
+struct DefectTable {
+  int n;
+  DefectDesc c[64];
+};
+
+template <int NC, int ND, typename T>
+__global__ void __launch_bounds__(256) multi_defect_sums_kernel(const __grid_constant__ DefectTable tab, double bnc,
+                                                                double *part) {
+  int lo = 0, hi = tab.n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (tab.c[mid].block_begin <= (int)blockIdx.x) lo = mid;
+    else hi = mid - 1;
+  }
+  const DefectDesc &c = tab.c[lo];
+  const int b = (int)blockIdx.x - c.block_begin;
+  defect_partial<NC, ND, T>(Links<NC, T>{(cx<T> *)c.links, c.g.V}, c.g, c.df, bnc, b,
+                            part + 2 * ((long long)c.part_begin + b));
+}
+
+__global__ void multi_defect_reduce_kernel(const __grid_constant__ DefectTable tab, const double *part, double *A) {
+  const int k = threadIdx.x;
+  if (k >= tab.n) return;
+  const DefectDesc &c = tab.c[k];
+  double a1 = 0.0, a2 = 0.0;
+  for (int b = 0; b < c.nblk; ++b) {
+    a1 += part[2 * ((long long)c.part_begin + b)];
+    a2 += part[2 * ((long long)c.part_begin + b) + 1];
+  }
+  A[2 * c.rep] = a1;
+  A[2 * c.rep + 1] = a2;
 }
 
 __global__ void defect_sums_reduce_kernel(const double *part, int nblk, double *out) {
@@ -118,6 +177,70 @@ cudaError_t launch_defect_sums(int nc, int dtype, const void *links, const Geom 
 
 // Sequential swap attempts of neighbouring labels (k, k+1), k = 0..nrep-2, on the
 // device (one thread): the same decision rule as the host path below.
+template <int NC, typename T>
+static cudaError_t launch_multi_defect_nc(int nd, const DefectTable &tab, int blocks, double bnc, double *part,
+                                          double *A, cudaStream_t st) {
+  if (nd == 2) multi_defect_sums_kernel<NC, 2, T><<<blocks, 256, 0, st>>>(tab, bnc, part);
+  else if (nd == 3) multi_defect_sums_kernel<NC, 3, T><<<blocks, 256, 0, st>>>(tab, bnc, part);
+  else multi_defect_sums_kernel<NC, 4, T><<<blocks, 256, 0, st>>>(tab, bnc, part);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  multi_defect_reduce_kernel<<<1, 64, 0, st>>>(tab, part, A);
+  return cudaGetLastError();
+}
+
+// A_1, A_2 of replica r into A[2r], A[2r + 1] for all replicas (at most 64),
+// one launch pair per (Nc, Nd, precision) group; part holds
+// 2 * multi_defect_parts(reps) doubles.
+cudaError_t enqueue_multi_defect_sums(const std::vector<klft_lattice *> &reps, double beta, double *part, double *A,
+                                      cudaStream_t st) {
+  if (reps.size() > 64) return cudaErrorInvalidValue;
+  std::vector<bool> done(reps.size(), false);
+  int pbeg = 0;
+  DefectTable tab;
+  for (size_t r0 = 0; r0 < reps.size(); ++r0) {
+    if (done[r0]) continue;
+    const klft_lattice *k = reps[r0];
+    std::memset(&tab, 0, sizeof(tab));
+    int blocks = 0;
+    for (size_t r = r0; r < reps.size(); ++r) {
+      const klft_lattice *l = reps[r];
+      if (done[r] || l->nc != k->nc || l->g.nd != k->g.nd || l->dtype() != k->dtype()) continue;
+      done[r] = true;
+      DefectDesc &d = tab.c[tab.n++];
+      d.links = l->links;
+      d.g = l->g;
+      d.df = l->defect;
+      d.rep = (int)r;
+      d.block_begin = blocks;
+      d.nblk = defect_sums_blocks(l->g);
+      d.part_begin = pbeg;
+      blocks += d.nblk;
+      pbeg += d.nblk;
+    }
+    const double bnc = beta / (double)k->nc;
+    const int nd = k->g.nd;
+    cudaError_t e;
+    if (k->dtype() == 0) {
+      if (k->nc == 1) e = launch_multi_defect_nc<1, double>(nd, tab, blocks, bnc, part, A, st);
+      else if (k->nc == 2) e = launch_multi_defect_nc<2, double>(nd, tab, blocks, bnc, part, A, st);
+      else e = launch_multi_defect_nc<3, double>(nd, tab, blocks, bnc, part, A, st);
+    } else {
+      if (k->nc == 1) e = launch_multi_defect_nc<1, float>(nd, tab, blocks, bnc, part, A, st);
+      else if (k->nc == 2) e = launch_multi_defect_nc<2, float>(nd, tab, blocks, bnc, part, A, st);
+      else e = launch_multi_defect_nc<3, float>(nd, tab, blocks, bnc, part, A, st);
+    }
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+long long multi_defect_parts(const std::vector<klft_lattice *> &reps) {
+  long long n = 0;
+  for (const klft_lattice *l : reps) n += defect_sums_blocks(l->g);
+  return n;
+}
+
 __global__ void ptbc_swap_kernel(int nrep, const double *c_of_label, const double *A, int *label_of_rep,
                                  int *rep_of_label, double *c_of_rep, uint64_t seed, const uint32_t *cycle_ctr,
                                  unsigned long long *swap_acc) {
