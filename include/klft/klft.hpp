@@ -6,6 +6,7 @@
 #pragma once
 
 #include <array>
+#include <complex>
 #include <cstddef>
 #include <string>
 #include <vector>
@@ -79,6 +80,12 @@ void WilsonLoop_mu_nu(klft_lattice *g, index_t mu, index_t nu, const std::vector
                       std::vector<std::array<real_t, 5>> &out);
 void WilsonLoop_temporal(klft_lattice *g, const std::vector<std::array<index_t, 2>> &pairs,
                          std::vector<std::array<real_t, 3>> &out);
+// GaugeVector.hpp:237-262 (legacy GaugeVector path): one Lmu x Lnu loop in the
+// (mu, nu) plane, mu != nu; Normalize divides the Re Tr sum by V * Nc
+real_t get_W_loop_mu_nu(klft_lattice *g, index_t mu, index_t nu, index_t Lmu, index_t Lnu, bool Normalize = true);
+// Gauge_Util.hpp:27-97: the staple of every link (periodic), complex128
+// [V][Nd][Nc][Nc], site = x0 + L0*(x1 + L1*(x2 + L2*x3)); empty on error
+std::vector<std::complex<double>> stapleField(klft_lattice *g);
 // Metropolis.hpp:118-178
 real_t sweep_Metropolis(klft_lattice *g, const MetropolisParams &p);
 // GaugeObservable.hpp:64-127 and :130-240

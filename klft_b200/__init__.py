@@ -154,6 +154,12 @@ class GaugeField:
                                            o.ctypes.data_as(C.POINTER(C.c_double))))
         return o
 
+    def wilson_loop(self, mu: int, nu: int, Lmu: int, Lnu: int, normalize: bool = True) -> float:
+        """One Lmu x Lnu loop in the (mu, nu) plane: klft's legacy get_W_loop_mu_nu
+        (GaugeVector.hpp:237-262); normalize=False gives the Re Tr sum over sites."""
+        w = float(self.wilson_loop_mu_nu(mu, nu, [(Lmu, Lnu)])[0])
+        return w if normalize else w * self.V * self.nc
+
     def wilson_loop_temporal(self, pairs) -> np.ndarray:
         p = _pairs(pairs)
         o = np.zeros(len(p))

@@ -204,6 +204,30 @@ void WilsonLoop_temporal(klft_lattice *g, const std::vector<std::array<index_t, 
   for (size_t k = 0; k < pairs.size(); ++k) out.push_back({(real_t)pairs[k][0], (real_t)pairs[k][1], w[k]});
 }
 
+real_t get_W_loop_mu_nu(klft_lattice *g, index_t mu, index_t nu, index_t Lmu, index_t Lnu, bool Normalize) {
+  const int pair[2] = {Lmu, Lnu};
+  double w = 0.0;
+  report(klft_wilson_loop_mu_nu(g, mu, nu, pair, 1, &w), "get_W_loop_mu_nu");
+  if (!Normalize) {
+    int nc = 0, nd = 0;
+    long long V = 0;
+    klft_lattice_info(g, &nc, &nd, nullptr, nullptr, &V);
+    w *= (double)V * (double)nc;
+  }
+  return w;
+}
+
+std::vector<std::complex<double>> stapleField(klft_lattice *g) {
+  int nc = 0, nd = 0;
+  long long V = 0;
+  report(klft_lattice_info(g, &nc, &nd, nullptr, nullptr, &V), "stapleField");
+  std::vector<std::complex<double>> out((size_t)V * nd * nc * nc);
+  const klft_status s = klft_staple_field(g, reinterpret_cast<double *>(out.data()));
+  report(s, "stapleField");
+  if (s != KLFT_OK) out.clear();
+  return out;
+}
+
 real_t sweep_Metropolis(klft_lattice *g, const MetropolisParams &p) {
   double acc = 0.0;
   report(klft_metropolis_sweeps(g, p.beta, p.delta, p.nHits, p.proposal, p.eps, 1, &acc), "sweep_Metropolis");

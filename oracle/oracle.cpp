@@ -463,6 +463,37 @@ template <int NC> static double wilson_mu_nu(const Field<NC> &F, int mu, int nu,
   return total.real();
 }
 
+// GaugeVector.hpp:237-262 (get_W_loop_mu_nu, the legacy GaugeVector path), as
+// its whole-field steps: set_one + wilson_line (:224-235, right-multiplication
+// along the direction), copy, shift_plus (:188-196, out(x) = in(x + dist e_d)),
+// UxU / UxUdag (:130-170) and sum_retrace (:213-222); Normalize divides by V*Nc.
+template <int NC>
+static double wilson_legacy(const Field<NC> &F, int mu, int nu, int Lmu, int Lnu, bool normalize) {
+  const Geo &g = F.g;
+  std::vector<Mat<NC>> U1(g.V), U2(g.V), U3, U4, tmp(g.V);
+  for (long s = 0; s < g.V; ++s) {
+    U1[s] = ident<NC>();
+    long y = s;
+    for (int i = 0; i < Lmu; ++i) { U1[s] = mul(U1[s], F.at(y, mu)); y = g.shift(y, mu, 1); }
+    U2[s] = ident<NC>();
+    y = s;
+    for (int i = 0; i < Lnu; ++i) { U2[s] = mul(U2[s], F.at(y, nu)); y = g.shift(y, nu, 1); }
+  }
+  U3 = U1;
+  U4 = U2;
+  for (long s = 0; s < g.V; ++s) tmp[s] = U2[g.shift(s, mu, Lmu)];
+  U2 = tmp;
+  for (long s = 0; s < g.V; ++s) U1[s] = mul(U1[s], U2[s]);
+  for (long s = 0; s < g.V; ++s) tmp[s] = U3[g.shift(s, nu, Lnu)];
+  U3 = tmp;
+  for (long s = 0; s < g.V; ++s) U1[s] = mul(U1[s], dag(U3[s]));
+  for (long s = 0; s < g.V; ++s) U1[s] = mul(U1[s], dag(U4[s]));
+  double W = 0.0;
+  for (long s = 0; s < g.V; ++s) W += trace(U1[s]).real();
+  if (normalize) W /= (double)g.V * (double)NC;
+  return W;
+}
+
 // Metropolis.hpp:73-113 (site functor), :118-178 (sublattice sweep, acceptance norm)
 template <int NC>
 static double metropolis_sweep(const Field<NC> &F, double beta, double delta, int nHits, int proposal, double eps,
@@ -833,6 +864,13 @@ int oracle_wilson_mu_nu(int nc, int nd, const int *L, const double *U, int mu, i
     Field<NC> F{g, (cplx *)U, nullptr};
     for (int k = 0; k < n; ++k) out[k] = wilson_mu_nu(F, mu, nu, pairs[2 * k], pairs[2 * k + 1]);
   }));
+  return 0;
+}
+
+int oracle_wilson_legacy(int nc, int nd, const int *L, const double *U, int mu, int nu, int Lmu, int Lnu,
+                         int normalize, double *out) {
+  Geo g(nd, L);
+  DISPATCH_NC(nc, (*out = wilson_legacy(Field<NC>{g, (cplx *)U, nullptr}, mu, nu, Lmu, Lnu, normalize != 0)));
   return 0;
 }
 

@@ -80,6 +80,8 @@ class Oracle:
         L.oracle_staple_field.argtypes = [C.c_int, C.c_int, _ip, _dp, _dp]
         L.oracle_plaquette.argtypes = [C.c_int, C.c_int, _ip, _dp, C.c_int, _dp]
         L.oracle_wilson_mu_nu.argtypes = [C.c_int, C.c_int, _ip, _dp, C.c_int, C.c_int, _ip, C.c_int, _dp]
+        L.oracle_wilson_legacy.argtypes = [C.c_int, C.c_int, _ip, _dp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                           _dp]
         L.oracle_wilson_temporal.argtypes = [C.c_int, C.c_int, _ip, _dp, _ip, C.c_int, _dp]
         L.oracle_metropolis.argtypes = [C.c_int, C.c_int, _ip, _dp, C.c_double, C.c_double, C.c_int, C.c_int,
                                         C.c_double, C.c_uint64, C.c_uint64, C.c_uint32, C.c_int, _ip, C.c_double,
@@ -141,6 +143,12 @@ class Oracle:
         o = np.zeros(len(p))
         self.lib.oracle_wilson_mu_nu(lat.nc, lat.nd, _i(lat.Lc), _d(U), mu, nu, _i(p), len(p), _d(o))
         return o
+
+    def wilson_legacy(self, lat: Lat, U, mu, nu, Lmu, Lnu, normalize=True):
+        """GaugeVector.hpp:237-262 get_W_loop_mu_nu, step by step over whole fields."""
+        o = np.zeros(1)
+        self.lib.oracle_wilson_legacy(lat.nc, lat.nd, _i(lat.Lc), _d(U), mu, nu, Lmu, Lnu, int(normalize), _d(o))
+        return float(o[0])
 
     def wilson_temporal(self, lat: Lat, U, pairs):
         p = np.ascontiguousarray(np.array(pairs, dtype=np.int32).reshape(-1, 2))

@@ -148,3 +148,26 @@ def test_su2_2d_exact_plaquette(oracle):
         oracle.metropolis(lat, U, beta, 0.4, 10, 1, 21, sweep0=100 + k)
         ps.append(oracle.plaquette(lat, U))
     assert np.mean(ps) == pytest.approx(iv(2, beta) / iv(1, beta), abs=0.01)
+
+
+@pytest.mark.parametrize("nd,nc", [(4, 3), (3, 2), (2, 1)])
+def test_legacy_gaugevector_loop_matches_wilson_mu_nu(oracle, nd, nc):
+    """The legacy whole-field path (GaugeVector.hpp:237-262) and the per-site
+    WilsonLoop_mu_nu restatement (pinned against klft's headers) agree on every
+    plane, for loops longer than the extent and with mu > nu; Normalize=false is
+    the Re Tr sum, V * Nc times the normalised value; identity links give 1."""
+    L = [4, 6, 4, 6][:nd]
+    lat = Lat(nc, L)
+    U = oracle.init(lat, True, 77)
+    V = int(np.prod(L))
+    for mu in range(nd):
+        for nu in range(nd):
+            if mu == nu:
+                continue
+            for Lmu, Lnu in [(1, 1), (2, 3), (5, 1), (0, 2)]:
+                w = oracle.wilson_legacy(lat, U, mu, nu, Lmu, Lnu)
+                ref = oracle.wilson_mu_nu(lat, U, mu, nu, [(Lmu, Lnu)])[0]
+                assert abs(w - ref) < 1e-13
+                raw = oracle.wilson_legacy(lat, U, mu, nu, Lmu, Lnu, normalize=False)
+                assert abs(raw - w * V * nc) < 1e-10 * V
+    assert abs(oracle.wilson_legacy(lat, oracle.init(lat, False), 0, nd - 1, 3, 2) - 1.0) < 1e-15
