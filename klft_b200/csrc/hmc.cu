@@ -44,15 +44,23 @@ __global__ void __launch_bounds__(HMC_THREADS) momenta_kernel(T *P, Geom g, uint
 
 // P -= dt * (beta/Nc) Adj(U S): the force of GaugeMonomial::derivative fused with
 // HamiltonianField::update_momentum; one thread per link.
+// Grid: x over the links of one direction, y = mu (so mu is uniform per CTA and
+// the staple's site arithmetic is compiled per direction).
 template <int NC, int ND, typename T>
 __global__ void __launch_bounds__(128) force_update_kernel(Links<NC, T> U, T *P, Geom g, T bnc, T dt) {
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= g.V * ND) return;
-  const int mu = (int)(t / g.V);
-  const long long lin = t - (long long)mu * g.V;
-  const Site x = site_from_lin(g, lin);
-  const Defect none{0, 1, {0, 0, 0}, 1.0, nullptr};
-  const Mat<NC, T> M = mul(U.load(lin, mu), staple<NC, ND, T>(U, g, x, mu, none));
+  const long long lin = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (lin >= g.V) return;
+  const int mu = (int)blockIdx.y;
+  const Site x = g.Vh < (1LL << 31) ? site_from_lin32(g, (unsigned)lin) : site_from_lin(g, lin);
+  Mat<NC, T> S;
+  if constexpr (NC == 3) {
+    // SU(3): the rolled staple (the unrolled products cost occupancy: 150 registers)
+    const Defect none{0, 1, {0, 0, 0}, 1.0, nullptr};
+    S = staple<NC, ND, T>(U, g, x, mu, none);
+  } else {
+    S = staple_dispatch<NC, ND, T>(U, g, x, mu);
+  }
+  const Mat<NC, T> M = mul(U.load(lin, mu), S);
   constexpr int nc = Alg<NC>::n;
   T v[nc];
   adjoint(M, v);
@@ -154,7 +162,7 @@ cudaError_t launch_momenta(const klft_lattice *lat, void *P) {
 cudaError_t launch_force_update(const klft_lattice *lat, void *P, double beta, double dt) {
   const Geom &g = lat->g;
 #define KLFT_FU(NDV)                                                                                        \
-  force_update_kernel<NC, NDV, T><<<grid_for(g.V * NDV, 128), 128, 0, lat->stream>>>(                       \
+  force_update_kernel<NC, NDV, T><<<dim3(grid_for(g.V, 128), NDV), 128, 0, lat->stream>>>(                   \
       Links<NC, T>{(cx<T> *)lat->links, g.V}, (T *)P, g, (T)(beta / (double)NC), (T)dt)
   KLFT_HMC_DISPATCH(lat->nc, lat->dtype(), ({
     if (g.nd == 2) KLFT_FU(2);

@@ -42,4 +42,60 @@ KLFT_D Mat<NC, T> staple(const Links<NC, T> &U, const Geom &g, const Site &x, in
   return S;
 }
 
+// The same staple with mu fixed at compile time and the nu loops unrolled: the
+// same products in the same order, but every site step and index folds to a few
+// integer operations.  For kernels without proposal code (the HMC force), where
+// the unrolled products fit the instruction cache.
+template <int NC, int ND, int MU, typename T>
+KLFT_D Mat<NC, T> staple_ct(const Links<NC, T> &U, const Geom &g, const Site &x) {
+  Mat<NC, T> S = mzero<NC, T>();
+  const Site xpmu = site_up(g, x, MU);
+#pragma unroll
+  for (int nu = 0; nu < ND; ++nu) {
+    if (nu == MU) continue;
+    const Site xpnu = site_up(g, x, nu);
+    const Mat<NC, T> t = mul_nd(U.load(site_lin(g, xpmu), nu), U.load(site_lin(g, xpnu), MU));
+    madd(S, mul_nd(t, U.load(site_lin(g, x), nu)));
+  }
+#pragma unroll
+  for (int nu = 0; nu < ND; ++nu) {
+    if (nu == MU) continue;
+    const Site xpmu_mnu = site_dn(g, xpmu, nu);
+    const Site xmnu = site_dn(g, x, nu);
+    const Mat<NC, T> t = mul_dd(U.load(site_lin(g, xpmu_mnu), nu), U.load(site_lin(g, xmnu), MU));
+    madd(S, mul(t, U.load(site_lin(g, xmnu), nu)));
+  }
+  return S;
+}
+
+// staple_ct for a run-time mu (uniform across a warp in the callers)
+template <int NC, int ND, typename T>
+KLFT_D Mat<NC, T> staple_dispatch(const Links<NC, T> &U, const Geom &g, const Site &x, int mu) {
+  if (mu == 0) return staple_ct<NC, ND, 0, T>(U, g, x);
+  if (mu == 1) return staple_ct<NC, ND, 1, T>(U, g, x);
+  if constexpr (ND > 2) {
+    if (mu == 2) return staple_ct<NC, ND, 2, T>(U, g, x);
+  }
+  if constexpr (ND > 3) return staple_ct<NC, ND, 3, T>(U, g, x);
+  return staple_ct<NC, ND, ND - 1, T>(U, g, x);
+}
+
+// Site of a class-blocked index lin = sub * Vh + hidx in 32-bit arithmetic
+// (lattices with Vh < 2^31).
+KLFT_D Site site_from_lin32(const Geom &g, unsigned lin) {
+  Site s;
+  const unsigned vh = (unsigned)g.Vh;
+  const unsigned sub = lin / vh;
+  unsigned hidx = lin - sub * vh;
+#pragma unroll
+  for (int d = 0; d < 4; ++d) {
+    const unsigned hd = (unsigned)g.H[d];
+    const unsigned q = hidx / hd;
+    s.set_b(d, (int)((sub >> d) & 1u));
+    s.set_h(d, (int)(hidx - q * hd));
+    hidx = q;
+  }
+  return s;
+}
+
 }  // namespace klft
