@@ -47,9 +47,9 @@ KLFT_HD long long window_threads(const Geom &g) { return (long long)(1 << g.nd) 
 template <typename T> struct PlaqMinBlocks { static constexpr int v = 2; };
 template <> struct PlaqMinBlocks<double> { static constexpr int v = 1; };
 
-// planes (mu, nu) with mu < nu < nu_end (nu_end = Nd: all planes)
-// One block's share of the plaquette sum: block b of nb over the window order
-// (the partial that plaquette_kernel's block b writes).
+// One block's share of the plaquette sum over the planes (mu, nu) with
+// mu < nu < nu_end (nu_end = Nd: all planes): block b of nb over the window
+// order (the partial that plaquette_kernel's block b writes).
 template <int NC, int ND, typename T>
 KLFT_D double plaquette_partial(const Links<NC, T> &U, const Geom &g, int nu_end, long long b, long long nb) {
   double acc = 0.0;
@@ -58,12 +58,14 @@ KLFT_D double plaquette_partial(const Links<NC, T> &U, const Geom &g, int nu_end
     Site x;
     long long lin;
     if (!window_site(g, t, x, lin)) continue;
-#pragma unroll 1
+    // unrolled over (mu, nu): the site steps fold to a few integer operations
+#pragma unroll
     for (int mu = 0; mu < ND; ++mu) {
       const Site xpmu = site_up(g, x, mu);
       const Mat<NC, T> umu = U.load(lin, mu);
-#pragma unroll 1
-      for (int nu = mu + 1; nu < nu_end; ++nu) {
+#pragma unroll
+      for (int nu = mu + 1; nu < ND; ++nu) {
+        if (nu >= nu_end) break;
         const Mat<NC, T> lmu = mul(umu, U.load(site_lin(g, xpmu), nu));
         const Mat<NC, T> lnu = mul(U.load(lin, nu), U.load(site_lin(g, site_up(g, x, nu)), mu));
         acc += retr_nd<NC, T, double>(lmu, lnu);

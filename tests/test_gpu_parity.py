@@ -148,7 +148,9 @@ def test_invalid_arguments_raise():
     with pytest.raises(klft_b200.KlftError):
         g.wilson_loop_mu_nu(0, 4, [(1, 1)])
     with pytest.raises(klft_b200.KlftError):
-        g.metropolis(1.0, 0.1, 1, 1, proposal="exp", eps=0.1) if False else g.wilson_loop_temporal([(-1, 2)])
+        g.wilson_loop_temporal([(-1, 2)])
+    with pytest.raises(klft_b200.KlftError):
+        g.metropolis(1.0, float("nan"), 1, 1)
     g.close()
 
 
