@@ -242,8 +242,12 @@ struct klft_batch {
     double beta, delta, eps;
     int nhits, proposal;
   };
+  static constexpr int NSIDE = 3;
   int device = 0;
   cudaStream_t stream = nullptr;
+  // side streams for the sweep launches of the second and later chain groups
+  cudaStream_t side[NSIDE] = {};
+  cudaEvent_t ev_fork = nullptr, ev_join[NSIDE] = {};
   std::vector<Chain> chains;
   // PTBC
   std::vector<int> reps;  // chain ids of the replicas, replica r = reps[r]
@@ -334,7 +338,7 @@ namespace klft {
 // index = items[i].acc_index (i when negative), stride = acc_stride (n when 0);
 // the caller advances the items' sweep counters afterwards.
 klft_status enqueue_multi_sweep(const std::vector<SweepItem> &items, unsigned long long *nacc, const uint32_t *slot,
-                                cudaStream_t st, int acc_stride, int *nlaunch) {
+                                cudaStream_t st, int acc_stride, int *nlaunch, const StreamFork *fork) {
   const int n = (int)items.size();
   const int stride = acc_stride > 0 ? acc_stride : n;
   std::vector<Group> groups;
@@ -369,14 +373,30 @@ klft_status enqueue_multi_sweep(const std::vector<SweepItem> &items, unsigned lo
   }
   int maxnd = 0;
   for (auto &gg : groups) maxnd = gg.key.nd > maxnd ? gg.key.nd : maxnd;
-  for (int val = 0; val < (1 << maxnd); ++val)
-    for (auto &gg : groups) {
+  const int ng = (int)groups.size();
+  const int nside = fork && ng > 1 ? std::min(fork->nside, ng - 1) : 0;
+  if (nside > 0) {
+    CK(cudaEventRecord(fork->fork, st));
+    for (int i = 0; i < nside; ++i) CK(cudaStreamWaitEvent(fork->side[i], fork->fork, 0));
+  }
+  // the side streams are joined back even when a launch fails
+  cudaError_t err = cudaSuccess;
+  for (int val = 0; val < (1 << maxnd) && err == cudaSuccess; ++val)
+    for (int gi = 0; gi < ng && err == cudaSuccess; ++gi) {
+      const Group &gg = groups[gi];
       if (val >= (1 << gg.key.nd)) continue;
-      for (size_t t = 0; t < gg.tables.size(); ++t) {
-        CK(launch_group(gg.key, *gg.tables[t], gg.blocks[t], val, nacc, slot, st));
+      const cudaStream_t gs = gi == 0 || nside == 0 ? st : fork->side[(gi - 1) % nside];
+      for (size_t t = 0; t < gg.tables.size() && err == cudaSuccess; ++t) {
+        err = launch_group(gg.key, *gg.tables[t], gg.blocks[t], val, nacc, slot, gs);
         if (nlaunch) ++*nlaunch;
       }
     }
+  for (int i = 0; i < nside; ++i) {
+    const cudaError_t e1 = cudaEventRecord(fork->join[i], fork->side[i]);
+    const cudaError_t e2 = cudaStreamWaitEvent(st, fork->join[i], 0);
+    if (err == cudaSuccess) err = e1 != cudaSuccess ? e1 : e2;
+  }
+  if (err != cudaSuccess) return cuda_fail(err, "enqueue_multi_sweep");
   return KLFT_OK;
 }
 
@@ -415,7 +435,9 @@ klft_status enqueue_cycle(klft_batch *b, int measure) {
       if (b->reps[r] == i) it.df.dyn_c = b->d_c_of_rep + r;
     items.push_back(it);
   }
-  klft_status st = enqueue_multi_sweep(items, (unsigned long long *)b->s_nacc.ptr, b->d_slot, b->stream, 0, nullptr);
+  const StreamFork fork{b->ev_fork, b->side, b->ev_join, klft_batch::NSIDE};
+  klft_status st =
+      enqueue_multi_sweep(items, (unsigned long long *)b->s_nacc.ptr, b->d_slot, b->stream, 0, nullptr, &fork);
   if (st != KLFT_OK) return st;
   CK(launch_advance_many(b->d_ctrs, n, b->stream));
   if (!b->reps.empty()) {
@@ -478,6 +500,11 @@ klft_status klft_batch_create(klft_batch **out) {
   klft_batch *b = new klft_batch();
   cudaGetDevice(&b->device);
   cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+  for (int i = 0; i < klft_batch::NSIDE && e == cudaSuccess; ++i) {
+    e = cudaStreamCreateWithFlags(&b->side[i], cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_join[i], cudaEventDisableTiming);
+  }
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaMalloc(&b->d_slot, 4 * sizeof(uint32_t));
   if (e == cudaSuccess) e = cudaMemsetAsync(b->d_slot, 0, 4 * sizeof(uint32_t), b->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
@@ -502,6 +529,11 @@ klft_status klft_batch_destroy(klft_batch *b) {
                     (void *)b->d_swap_acc})
       if (p) cudaFree(p);
     if (b->stream) cudaStreamDestroy(b->stream);
+    for (int i = 0; i < klft_batch::NSIDE; ++i) {
+      if (b->side[i]) cudaStreamDestroy(b->side[i]);
+      if (b->ev_join[i]) cudaEventDestroy(b->ev_join[i]);
+    }
+    if (b->ev_fork) cudaEventDestroy(b->ev_fork);
   }
   delete b;
   return KLFT_OK;

@@ -71,8 +71,18 @@ struct SweepItem {
   Defect df;
   int acc_index;  // accept-counter index; < 0: the item's position
 };
+// Side streams for enqueue_multi_sweep: the chains of different launch groups
+// share no data, so group g > 0 may run on side[(g - 1) % nside], forked from
+// and joined back into the main stream with the given events (also inside a
+// stream capture, where the fork and join become graph edges).
+struct StreamFork {
+  cudaEvent_t fork;
+  const cudaStream_t *side;
+  const cudaEvent_t *join;  // one per side stream
+  int nside;
+};
 klft_status enqueue_multi_sweep(const std::vector<SweepItem> &items, unsigned long long *nacc, const uint32_t *slot,
-                                cudaStream_t st, int acc_stride, int *nlaunch);
+                                cudaStream_t st, int acc_stride, int *nlaunch, const StreamFork *fork = nullptr);
 // sweep counters += 1: a device array of counter pointers, or a host list
 cudaError_t launch_advance_many(uint32_t *const *d_ctrs, int n, cudaStream_t st);
 cudaError_t launch_advance_list(const std::vector<uint32_t *> &ctrs, cudaStream_t st, int *nlaunch);
