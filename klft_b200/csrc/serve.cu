@@ -191,6 +191,23 @@ struct klft_server {
   std::thread worker;
   cudaStream_t stream = nullptr;  // class 0 (and server-level work)
   cudaStream_t cls_stream[kClasses] = {};
+  // per class: side streams for the second and later launch groups of a round
+  // step (jobs of different Nc, Nd, precision or proposal share no data)
+  static constexpr int kSide = 2;
+  cudaStream_t side[kClasses][kSide] = {};
+  cudaEvent_t ev_fork[kClasses] = {}, ev_join[kClasses][kSide] = {};
+  void destroy_side() {
+    for (int k = 0; k < kClasses; ++k) {
+      for (int i = 0; i < kSide; ++i) {
+        if (side[k][i]) cudaStreamDestroy(side[k][i]);
+        if (ev_join[k][i]) cudaEventDestroy(ev_join[k][i]);
+        side[k][i] = nullptr;
+        ev_join[k][i] = nullptr;
+      }
+      if (ev_fork[k]) cudaEventDestroy(ev_fork[k]);
+      ev_fork[k] = nullptr;
+    }
+  }
   unsigned long long *d_nacc = nullptr, *h_nacc = nullptr;
   uint32_t *d_zero = nullptr;
   std::vector<int> free_slots;
@@ -408,7 +425,8 @@ bool klft_server::enqueue_round(int cls) {
       }
     if (items.empty()) break;
     int nl = 0;
-    klft_status s = enqueue_multi_sweep(items, d_nacc, d_zero, stream, max_active, &nl);
+    const StreamFork fork{ev_fork[cls], side[cls], ev_join[cls], kSide};
+    klft_status s = enqueue_multi_sweep(items, d_nacc, d_zero, stream, max_active, &nl, &fork);
     if (s != KLFT_OK) throw std::runtime_error(klft_last_error());
     cudaError_t e = launch_advance_list(ctrs, stream, &nl);
     if (e != cudaSuccess) throw std::runtime_error(cudaGetErrorString(e));
@@ -594,6 +612,13 @@ klft_status klft_server_create(int device, uint64_t budget_bytes, int max_active
   s->cls_stream[0] = s->stream;
   for (int k = 1; k < kClasses && e == cudaSuccess; ++k)
     e = cudaStreamCreateWithFlags(&s->cls_stream[k], cudaStreamNonBlocking);
+  for (int k = 0; k < kClasses && e == cudaSuccess; ++k) {
+    e = cudaEventCreateWithFlags(&s->ev_fork[k], cudaEventDisableTiming);
+    for (int i = 0; i < klft_server::kSide && e == cudaSuccess; ++i) {
+      e = cudaStreamCreateWithFlags(&s->side[k][i], cudaStreamNonBlocking);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_join[k][i], cudaEventDisableTiming);
+    }
+  }
   if (e == cudaSuccess) e = cudaMalloc(&s->d_nacc, (size_t)s->max_active * sizeof(unsigned long long));
   if (e == cudaSuccess) e = cudaMallocHost(&s->h_nacc, (size_t)s->max_active * sizeof(unsigned long long));
   if (e == cudaSuccess) e = cudaMalloc(&s->d_zero, 16);
@@ -603,6 +628,7 @@ klft_status klft_server_create(int device, uint64_t budget_bytes, int max_active
     if (s->d_nacc) cudaFree(s->d_nacc);
     if (s->h_nacc) cudaFreeHost(s->h_nacc);
     if (s->d_zero) cudaFree(s->d_zero);
+    s->destroy_side();
     for (int k = 1; k < kClasses; ++k)
       if (s->cls_stream[k]) cudaStreamDestroy(s->cls_stream[k]);
     if (s->stream) cudaStreamDestroy(s->stream);
@@ -635,6 +661,7 @@ klft_status klft_server_destroy(klft_server *s) {
   if (s->d_nacc) cudaFree(s->d_nacc);
   if (s->h_nacc) cudaFreeHost(s->h_nacc);
   if (s->d_zero) cudaFree(s->d_zero);
+  s->destroy_side();
   for (int k = 1; k < kClasses; ++k)
     if (s->cls_stream[k]) cudaStreamDestroy(s->cls_stream[k]);
   if (s->stream) cudaStreamDestroy(s->stream);
