@@ -43,7 +43,7 @@ def test_batch_equals_chains_alone(use_graph):
         for c in range(ncyc):
             a = solo_fields[k].metropolis(beta, delta, nh, 1, prop, eps)[0]
             assert acc[c, k] == a
-            assert plaq[c, k] == pytest.approx(solo_fields[k].plaquette(), rel=1e-12, abs=1e-14)
+            assert plaq[c, k] == solo_fields[k].plaquette()  # the single-lattice partials and order
         np.testing.assert_array_equal(batch_fields[k].download(), solo_fields[k].download())
         assert batch_fields[k].counters() == solo_fields[k].counters()
     # a second run continues every chain
