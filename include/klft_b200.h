@@ -158,6 +158,16 @@ klft_status klft_ptbc_defect_sums(klft_lattice *lat, double beta, double *out2);
  * decisions, and every replica's defect takes its new label's coefficient. */
 klft_status klft_ptbc_swap(klft_lattice *const *reps, int nrep, const double *c_of_label, int *label_of_rep,
                            double beta, uint64_t seed, uint32_t cycle, int *accepted);
+/* The swap decisions of klft_ptbc_swap from defect sums alone, on the host (no
+ * device work): A[2r], A[2r+1] = out2 of klft_ptbc_defect_sums for replica r.
+ * Same decisions and random stream as klft_ptbc_swap.  For replicas spread over
+ * processes or GPUs: every rank computes its replicas' sums, the sums are
+ * all-gathered (one FP64 pair per replica), and every rank calls this with the
+ * same arguments, so all ranks agree on the new labels without moving links. */
+klft_status klft_ptbc_swap_sums(const double *A, int nrep, const double *c_of_label, int *label_of_rep,
+                                uint64_t seed, uint32_t cycle, int *accepted);
+/* Coefficient c of an existing defect (EINVAL when the lattice has none). */
+klft_status klft_lattice_set_defect_c(klft_lattice *lat, double c);
 
 /* ---------------------------------------------------------------- batches
  * No counterpart in the reference (which runs one lattice per process): many

@@ -238,6 +238,10 @@ class GaugeField:
         p = (C.c_int * 3)(*(list(pos) + [0, 0, 0])[:3])
         check(lib().klft_lattice_set_defect(self._h, length, p, c))
 
+    def set_defect_c(self, c: float) -> None:
+        """Coefficient of the existing defect (a PTBC replica's new label)."""
+        check(lib().klft_lattice_set_defect_c(self._h, c))
+
     def defect_sums(self, beta: float) -> np.ndarray:
         o = np.zeros(2)
         check(lib().klft_ptbc_defect_sums(self._h, beta, o.ctypes.data_as(C.POINTER(C.c_double))))
@@ -262,6 +266,20 @@ def ptbc_swap(fields: Sequence[GaugeField], c_of_label, label_of_rep, beta: floa
     check(lib().klft_ptbc_swap(reps, n, c.ctypes.data_as(C.POINTER(C.c_double)),
                                lab.ctypes.data_as(C.POINTER(C.c_int)), beta, seed, cycle,
                                acc.ctypes.data_as(C.POINTER(C.c_int))))
+    return lab, acc[: n - 1]
+
+
+def ptbc_swap_sums(A, c_of_label, label_of_rep, seed: int, cycle: int):
+    """Swap decisions from defect sums A[r] = (A_1, A_2) of replica r, on the host
+    (klft_ptbc_swap_sums); returns (labels, accepted)."""
+    a = np.ascontiguousarray(A, dtype=np.float64).reshape(-1)
+    n = a.size // 2
+    c = np.ascontiguousarray(c_of_label, dtype=np.float64)
+    lab = np.ascontiguousarray(label_of_rep, dtype=np.int32).copy()
+    acc = np.zeros(max(n - 1, 1), dtype=np.int32)
+    check(lib().klft_ptbc_swap_sums(a.ctypes.data_as(C.POINTER(C.c_double)), n, c.ctypes.data_as(C.POINTER(C.c_double)),
+                                    lab.ctypes.data_as(C.POINTER(C.c_int)), seed, cycle,
+                                    acc.ctypes.data_as(C.POINTER(C.c_int))))
     return lab, acc[: n - 1]
 
 

@@ -94,6 +94,8 @@ SIGNATURES = {
     "klft_tuner_clear": (C.c_int, []),
     "klft_ptbc_defect_sums": (C.c_int, [_vp, C.c_double, _dp]),
     "klft_ptbc_swap": (C.c_int, [C.POINTER(_vp), C.c_int, _dp, _ip, C.c_double, C.c_uint64, C.c_uint32, _ip]),
+    "klft_ptbc_swap_sums": (C.c_int, [_dp, C.c_int, _dp, _ip, C.c_uint64, C.c_uint32, _ip]),
+    "klft_lattice_set_defect_c": (C.c_int, [_vp, C.c_double]),
     "klft_checkpoint_write": (C.c_int, [_vp, C.c_char_p]),
     "klft_checkpoint_read": (C.c_int, [C.c_char_p, C.POINTER(_vp)]),
     "klft_job_footprint": (C.c_int, [C.POINTER(Job), C.POINTER(C.c_uint64)]),

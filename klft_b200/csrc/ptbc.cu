@@ -314,21 +314,15 @@ klft_status klft_ptbc_defect_sums(klft_lattice *lat, double beta, double *out2) 
   return KLFT_OK;
 }
 
-klft_status klft_ptbc_swap(klft_lattice *const *reps, int nrep, const double *c_of_label, int *label_of_rep,
-                           double beta, uint64_t seed, uint32_t cycle, int *accepted) {
-  if (!reps || !c_of_label || !label_of_rep || nrep < 1) return fail(KLFT_EINVAL, "klft_ptbc_swap: bad arguments");
+klft_status klft_ptbc_swap_sums(const double *A, int nrep, const double *c_of_label, int *label_of_rep,
+                                uint64_t seed, uint32_t cycle, int *accepted) {
+  if (!A || !c_of_label || !label_of_rep || nrep < 1) return fail(KLFT_EINVAL, "klft_ptbc_swap_sums: bad arguments");
   std::vector<int> seen(nrep, 0), rep_of_label(nrep);
   for (int r = 0; r < nrep; ++r) {
-    if (!reps[r]) return fail(KLFT_EINVAL, "klft_ptbc_swap: null replica %d", r);
     const int l = label_of_rep[r];
-    if (l < 0 || l >= nrep || seen[l]) return fail(KLFT_EINVAL, "klft_ptbc_swap: labels are not a permutation");
+    if (l < 0 || l >= nrep || seen[l]) return fail(KLFT_EINVAL, "klft_ptbc_swap_sums: labels are not a permutation");
     seen[l] = 1;
     rep_of_label[l] = r;
-  }
-  std::vector<double> A(2 * (size_t)nrep);
-  for (int r = 0; r < nrep; ++r) {
-    klft_status s = klft_ptbc_defect_sums(reps[r], beta, &A[2 * r]);
-    if (s != KLFT_OK) return s;
   }
   for (int k = 0; k + 1 < nrep; ++k) {
     const int a = rep_of_label[k], b = rep_of_label[k + 1];
@@ -349,6 +343,35 @@ klft_status klft_ptbc_swap(klft_lattice *const *reps, int nrep, const double *c_
       label_of_rep[b] = k;
     }
   }
+  return KLFT_OK;
+}
+
+klft_status klft_lattice_set_defect_c(klft_lattice *lat, double c) {
+  if (!lat) return fail(KLFT_EINVAL, "klft_lattice_set_defect_c: null handle");
+  if (!(c == c)) return fail(KLFT_EINVAL, "klft_lattice_set_defect_c: NaN coefficient");
+  std::lock_guard<std::mutex> guard(lat->mtx);
+  if (!lat->defect.active) return fail(KLFT_EINVAL, "klft_lattice_set_defect_c: the lattice has no defect");
+  lat->defect.c = c;
+  return KLFT_OK;
+}
+
+klft_status klft_ptbc_swap(klft_lattice *const *reps, int nrep, const double *c_of_label, int *label_of_rep,
+                           double beta, uint64_t seed, uint32_t cycle, int *accepted) {
+  if (!reps || !c_of_label || !label_of_rep || nrep < 1) return fail(KLFT_EINVAL, "klft_ptbc_swap: bad arguments");
+  std::vector<int> seen(nrep, 0);
+  for (int r = 0; r < nrep; ++r) {
+    if (!reps[r]) return fail(KLFT_EINVAL, "klft_ptbc_swap: null replica %d", r);
+    const int l = label_of_rep[r];
+    if (l < 0 || l >= nrep || seen[l]) return fail(KLFT_EINVAL, "klft_ptbc_swap: labels are not a permutation");
+    seen[l] = 1;
+  }
+  std::vector<double> A(2 * (size_t)nrep);
+  for (int r = 0; r < nrep; ++r) {
+    klft_status s = klft_ptbc_defect_sums(reps[r], beta, &A[2 * r]);
+    if (s != KLFT_OK) return s;
+  }
+  klft_status s = klft_ptbc_swap_sums(A.data(), nrep, c_of_label, label_of_rep, seed, cycle, accepted);
+  if (s != KLFT_OK) return s;
   // every replica's defect carries its (new) label's coefficient
   for (int r = 0; r < nrep; ++r) {
     std::lock_guard<std::mutex> guard(reps[r]->mtx);
