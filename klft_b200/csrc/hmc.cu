@@ -242,7 +242,7 @@ klft_status enqueue_energies(klft_lattice *lat, const HmcBufs &b, double *slot_k
   const int nblk = plaquette_blocks(lat->g);
   CK(launch_kinetic(lat, b.P, (double *)lat->s_part.ptr, nblk, slot_k));
   CK(launch_plaquette(lat->nc, lat->dtype(), lat->links, lat->g, (double *)lat->s_part.ptr, nblk, slot_p,
-                      lat->stream));
+                      lat->stream, -1, true));
   return KLFT_OK;
 }
 

@@ -32,9 +32,10 @@ cudaError_t launch_unitarity(int nc, int dtype, const void *links, const Geom &g
 // staples of every link, written in host AoS FP64 layout
 cudaError_t launch_staple_field(int nc, int dtype, const void *links, const Geom &g, double *aos, cudaStream_t st);
 
-// sum over sites of sum_{mu<nu<nu_end} Re Tr P_{mu nu} (nu_end < 0: all planes), unnormalised, into *d_out
+// sum over sites of sum_{mu<nu<nu_end} Re Tr P_{mu nu} (nu_end < 0: all planes), unnormalised, into *d_out;
+// f64_terms: every product term summed in FP64 (else each plane's trace in the link precision)
 cudaError_t launch_plaquette(int nc, int dtype, const void *links, const Geom &g, double *d_part, int nblk,
-                             double *d_out, cudaStream_t st, int nu_end = -1);
+                             double *d_out, cudaStream_t st, int nu_end = -1, bool f64_terms = false);
 // Wilson loops of a pair list in the (mu, nu) plane; d_out[k] = sum over sites Re Tr W
 cudaError_t launch_wilson_direct(int nc, int dtype, const void *links, const Geom &g, int mu, int nu,
                                  const int *d_pairs, int npairs, double *d_part, int nblk, double *d_out,

@@ -16,10 +16,11 @@
 
 namespace klft {
 
-template <int NC, int ND, typename T>
+template <int NC, int ND, typename T, bool F64>
 __global__ void __launch_bounds__(RED_THREADS, PlaqMinBlocks<T>::v) plaquette_kernel(Links<NC, T> U, Geom g,
                                                                                      double *part, int nu_end) {
-  const double s = block_sum<RED_THREADS>(plaquette_partial<NC, ND, T>(U, g, nu_end, blockIdx.x, gridDim.x));
+  const double s =
+      block_sum<RED_THREADS>(plaquette_partial<NC, ND, T, F64>(U, g, nu_end, blockIdx.x, gridDim.x));
   if (threadIdx.x == 0) part[blockIdx.x] = s;
 }
 
@@ -101,10 +102,17 @@ cudaError_t launch_reduce_partials(const double *d_part, int nblk, int n, double
   } while (0)
 
 cudaError_t launch_plaquette(int nc, int dtype, const void *links, const Geom &g, double *d_part, int nblk,
-                             double *d_out, cudaStream_t st, int nu_end) {
+                             double *d_out, cudaStream_t st, int nu_end, bool f64_terms) {
   if (nu_end < 0) nu_end = g.nd;
-#define KLFT_PQ(NDV) \
-  plaquette_kernel<NC, NDV, T><<<nblk, RED_THREADS, 0, st>>>(Links<NC, T>{(cx<T> *)links, g.V}, g, d_part, nu_end)
+#define KLFT_PQ(NDV)                                                                                              \
+  do {                                                                                                            \
+    if (f64_terms)                                                                                                \
+      plaquette_kernel<NC, NDV, T, true><<<nblk, RED_THREADS, 0, st>>>(Links<NC, T>{(cx<T> *)links, g.V}, g,      \
+                                                                       d_part, nu_end);                           \
+    else                                                                                                          \
+      plaquette_kernel<NC, NDV, T, false><<<nblk, RED_THREADS, 0, st>>>(Links<NC, T>{(cx<T> *)links, g.V}, g,     \
+                                                                        d_part, nu_end);                          \
+  } while (0)
   KLFT_OBS_DISPATCH(nc, dtype, g.nd, ({
     if (g.nd == 2) KLFT_PQ(2);
     else if (g.nd == 3) KLFT_PQ(3);

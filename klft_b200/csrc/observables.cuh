@@ -50,7 +50,10 @@ template <> struct PlaqMinBlocks<double> { static constexpr int v = 1; };
 // One block's share of the plaquette sum over the planes (mu, nu) with
 // mu < nu < nu_end (nu_end = Nd: all planes): block b of nb over the window
 // order (the partial that plaquette_kernel's block b writes).
-template <int NC, int ND, typename T>
+// F64 = true sums every product term in FP64 (the HMC action, whose differences
+// decide acceptance); otherwise each plane's trace is formed in the link
+// precision and the lattice sum in FP64.
+template <int NC, int ND, typename T, bool F64 = false>
 KLFT_D double plaquette_partial(const Links<NC, T> &U, const Geom &g, int nu_end, long long b, long long nb) {
   double acc = 0.0;
   const long long nthr = window_threads(g);
@@ -68,7 +71,8 @@ KLFT_D double plaquette_partial(const Links<NC, T> &U, const Geom &g, int nu_end
         if (nu >= nu_end) break;
         const Mat<NC, T> lmu = mul(umu, U.load(site_lin(g, xpmu), nu));
         const Mat<NC, T> lnu = mul(U.load(lin, nu), U.load(site_lin(g, site_up(g, x, nu)), mu));
-        acc += retr_nd<NC, T, double>(lmu, lnu);
+        if constexpr (F64) acc += retr_nd<NC, T, double>(lmu, lnu);
+        else acc += (double)retr_nd<NC, T, T>(lmu, lnu);
       }
     }
   }
