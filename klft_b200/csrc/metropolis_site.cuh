@@ -67,11 +67,9 @@ KLFT_D void box_muller(uint32_t wa, uint32_t wb, float &g0, float &g1) {
   g1 = -r * s;
 }
 
+// X = exp(i eps H) of one hit from its eight stream words (blocks 2h, 2h+1)
 template <typename T>
-KLFT_D Mat<3, T> exp_proposal(const ExpHitStream &hs, uint32_t h, T half_eps) {
-  uint32_t w[8];
-  hs.block(2 * h, w);
-  hs.block(2 * h + 1, w + 4);
+KLFT_D Mat<3, T> exp_proposal_w(const uint32_t (&w)[8], T half_eps) {
   T g[8];
 #pragma unroll
   for (int k = 0; k < 4; ++k) box_muller(w[2 * k], w[2 * k + 1], g[2 * k], g[2 * k + 1]);
@@ -183,11 +181,22 @@ KLFT_D int site_update_exp(const Links<3, T> &U, const Geom &g, const Site &x, c
     T trO = retr_diag(M);
     bool changed = false;
     uint32_t aw[4];
+    // the Philox words of hit h + 1 are drawn while hit h is evaluated
+    uint32_t wn[8];
+    hs.block(2 * h0, wn);
+    hs.block(2 * h0 + 1, wn + 4);
 #pragma unroll 1
     for (int hit = 0; hit < a.nhits; ++hit) {
       const uint32_t h = h0 + (uint32_t)hit;
       if (hit == 0 || (h & 3u) == 0u) hs.accept_block(h, aw);
-      const Mat<3, T> rr = exp_proposal<T>(hs, h, half_eps);
+      uint32_t w[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) w[k] = wn[k];
+      if (hit + 1 < a.nhits) {
+        hs.block(2 * (h + 1), wn);
+        hs.block(2 * (h + 1) + 1, wn + 4);
+      }
+      const Mat<3, T> rr = exp_proposal_w<T>(w, half_eps);
       T dS = -bnc * (retr_mul(rr, M) - trO);
       if (dlink) dS *= (T)defect_c(df);
       const bool accept = dS < T(0) || accept_word(aw, h) < (double)exp(-dS);
