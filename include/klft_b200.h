@@ -29,7 +29,8 @@ typedef enum {
   KLFT_EINVAL = 1,   /* bad argument                        */
   KLFT_ENOMEM = 2,   /* device or host allocation failed    */
   KLFT_ECUDA = 3,    /* CUDA runtime error / no device      */
-  KLFT_ETIMEOUT = 4, /* a bounded device wait gave up       */
+  KLFT_ETIMEOUT = 4, /* a bounded wait gave up (reserved: no
+                      * kernel here waits on a flag or a peer) */
   KLFT_ENOTSUP = 5,  /* combination not supported           */
   KLFT_ECANCELED = 6, /* serving: the job was cancelled     */
   KLFT_EINTERNAL = 7, /* serving: the worker failed          */
