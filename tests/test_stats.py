@@ -47,3 +47,12 @@ def test_compare_independent_chains():
     assert abs(c["z"]) < 3
     c2 = compare(a + 0.5, b)
     assert c2["z"] > 5
+
+
+def test_ensemble_summary_is_the_standard_error_of_chain_means():
+    from klft_b200.ensemble import summary
+    rng = np.random.default_rng(3)
+    means = 0.59 + 1e-4 * rng.normal(size=4000)
+    m, e = summary(means)
+    assert abs(m - 0.59) < 5 * e
+    assert abs(e - 1e-4 / np.sqrt(4000)) < 0.1 * e
