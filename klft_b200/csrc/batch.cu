@@ -15,6 +15,7 @@
 // run on the device (ptbc.cu) and write each replica's defect coefficient,
 // which the sweep kernels read through Defect::dyn_c.
 #include <algorithm>
+#include <cstdio>
 #include <cstring>
 #include <memory>
 #include <vector>
@@ -24,6 +25,7 @@
 #include "kernels.cuh"
 #include "metropolis_site.cuh"
 #include "observables.cuh"
+#include "tuner.h"
 
 namespace klft {
 
@@ -42,6 +44,7 @@ struct ChainDesc {
 struct ChainTable {
   int n;
   int nchains_total;
+  int block;  // threads per CTA of the launch (<= 128)
   ChainDesc c[BATCH_MAX];
 };
 
@@ -260,7 +263,8 @@ struct klft_batch {
   double *d_c_of_label = nullptr, *d_c_of_rep = nullptr, *d_A = nullptr, *d_part = nullptr;
   int *d_label_of_rep = nullptr, *d_rep_of_label = nullptr;
   unsigned long long *d_swap_acc = nullptr;
-  klft::Scratch s_nacc, s_plaq, s_labels, s_ppart;
+  klft::Scratch s_nacc, s_plaq, s_labels, s_ppart, s_tune;
+  int sweep_block = 128;  // threads per CTA of the sweep launches (tuned under KLFT_TUNING)
   int cap = 0;  // result slots
   bool dirty = true;
   cudaGraph_t graph = nullptr;
@@ -288,7 +292,7 @@ struct GroupKey {
 template <int NC, int ND, typename T, bool EXP, bool DF>
 cudaError_t launch_group_t(const ChainTable &tab, int blocks, int val, unsigned long long *nacc, const uint32_t *slot,
                            cudaStream_t st) {
-  multi_pass_kernel<NC, ND, T, EXP, DF><<<blocks, 128, 0, st>>>(tab, val, nacc, slot);
+  multi_pass_kernel<NC, ND, T, EXP, DF><<<blocks, tab.block, 0, st>>>(tab, val, nacc, slot);
   return cudaGetLastError();
 }
 
@@ -338,7 +342,8 @@ namespace klft {
 // index = items[i].acc_index (i when negative), stride = acc_stride (n when 0);
 // the caller advances the items' sweep counters afterwards.
 klft_status enqueue_multi_sweep(const std::vector<SweepItem> &items, unsigned long long *nacc, const uint32_t *slot,
-                                cudaStream_t st, int acc_stride, int *nlaunch, const StreamFork *fork) {
+                                cudaStream_t st, int acc_stride, int *nlaunch, const StreamFork *fork, int block) {
+  if (block != 32 && block != 64 && block != 128) return fail(KLFT_EINVAL, "enqueue_multi_sweep: block %d", block);
   const int n = (int)items.size();
   const int stride = acc_stride > 0 ? acc_stride : n;
   std::vector<Group> groups;
@@ -358,6 +363,7 @@ klft_status enqueue_multi_sweep(const std::vector<SweepItem> &items, unsigned lo
       grp->tables.emplace_back(new ChainTable());
       std::memset(grp->tables.back().get(), 0, sizeof(ChainTable));
       grp->tables.back()->nchains_total = stride;
+      grp->tables.back()->block = block;
       grp->blocks.push_back(0);
     }
     ChainTable &tab = *grp->tables.back();
@@ -369,7 +375,7 @@ klft_status enqueue_multi_sweep(const std::vector<SweepItem> &items, unsigned lo
     d.df = it.df;
     d.index = it.acc_index >= 0 ? it.acc_index : i;
     d.block_begin = grp->blocks.back();
-    grp->blocks.back() += (int)((lat->g.Vh + 127) / 128);
+    grp->blocks.back() += (int)((lat->g.Vh + block - 1) / block);
   }
   int maxnd = 0;
   for (auto &gg : groups) maxnd = gg.key.nd > maxnd ? gg.key.nd : maxnd;
@@ -422,8 +428,8 @@ cudaError_t launch_advance_list(const std::vector<uint32_t *> &ctrs, cudaStream_
 
 namespace {
 
-// Enqueue one cycle on b->stream (recorded into the graph by the caller).
-klft_status enqueue_cycle(klft_batch *b, int measure) {
+// The sweep items of every chain (replicas read their coefficient from the device).
+std::vector<SweepItem> sweep_items(const klft_batch *b) {
   const int n = (int)b->chains.size();
   std::vector<SweepItem> items;
   for (int i = 0; i < n; ++i) {
@@ -435,9 +441,16 @@ klft_status enqueue_cycle(klft_batch *b, int measure) {
       if (b->reps[r] == i) it.df.dyn_c = b->d_c_of_rep + r;
     items.push_back(it);
   }
+  return items;
+}
+
+// Enqueue one cycle on b->stream (recorded into the graph by the caller).
+klft_status enqueue_cycle(klft_batch *b, int measure) {
+  const int n = (int)b->chains.size();
+  const std::vector<SweepItem> items = sweep_items(b);
   const StreamFork fork{b->ev_fork, b->side, b->ev_join, klft_batch::NSIDE};
-  klft_status st =
-      enqueue_multi_sweep(items, (unsigned long long *)b->s_nacc.ptr, b->d_slot, b->stream, 0, nullptr, &fork);
+  klft_status st = enqueue_multi_sweep(items, (unsigned long long *)b->s_nacc.ptr, b->d_slot, b->stream, 0, nullptr,
+                                       &fork, b->sweep_block);
   if (st != KLFT_OK) return st;
   CK(launch_advance_many(b->d_ctrs, n, b->stream));
   if (!b->reps.empty()) {
@@ -462,6 +475,73 @@ klft_status enqueue_cycle(klft_batch *b, int measure) {
                                b->stream, nullptr));
   }
   batch_slot_kernel<<<1, 1, 0, b->stream>>>(b->d_slot, b->d_slot + 1);
+  CK(cudaGetLastError());
+  return KLFT_OK;
+}
+
+// Under KLFT_TUNING: the CTA size of the batch's sweep launches (32, 64 or 128
+// threads), tuned once per batch composition (key: chain count and a hash of
+// every chain's group, extents, precision, proposal and defect) and cached like
+// the single-lattice sweep.  Candidates are timed on the chains' own links,
+// which are backed up first and restored afterwards; counters do not move, so
+// no chain is perturbed.  Results never depend on the block size.
+klft_status tune_sweep_block(klft_batch *b) {
+  b->sweep_block = 128;
+  if (!tuner_enabled()) return KLFT_OK;
+  const int n = (int)b->chains.size();
+  uint64_t h = 1469598103934665603ull;
+  auto mix = [&h](long long v) {
+    h ^= (uint64_t)v;
+    h *= 1099511628211ull;
+  };
+  long long sites = 0;
+  size_t total = 0;
+  for (const auto &ch : b->chains) {
+    const klft_lattice *l = ch.lat;
+    mix(l->nc);
+    mix(l->g.nd);
+    for (int d = 0; d < 4; ++d) mix(l->g.L[d]);
+    mix(l->dtype());
+    mix(ch.proposal);
+    mix(l->defect.active);
+    sites += l->g.Vh;
+    total += (l->link_bytes + 255) & ~(size_t)255;
+  }
+  char hex[17];
+  snprintf(hex, sizeof hex, "%016llx", (unsigned long long)h);
+  const std::string id = "sweep_Metropolis_batch_" + std::to_string(n) + "_chains_" + hex;
+  const int end[1] = {(int)std::min<long long>(sites, 2147483647LL)};
+  const std::string key = tune_key(id, 1, end);
+  const std::vector<SweepItem> items = sweep_items(b);
+  auto time_fn = [&](int block) -> float {
+    if (b->s_tune.ensure(total) != cudaSuccess) return -1.f;
+    char *bak = (char *)b->s_tune.ptr;
+    size_t off = 0;
+    for (const auto &ch : b->chains) {
+      if (cudaMemcpyAsync(bak + off, ch.lat->links, ch.lat->link_bytes, cudaMemcpyDeviceToDevice, b->stream) !=
+          cudaSuccess)
+        return -1.f;
+      off += (ch.lat->link_bytes + 255) & ~(size_t)255;
+    }
+    if (cudaMemsetAsync(b->d_slot, 0, sizeof(uint32_t), b->stream) != cudaSuccess) return -1.f;
+    const float ms = time_launches(b->stream, 3, [&] {
+      return enqueue_multi_sweep(items, (unsigned long long *)b->s_nacc.ptr, b->d_slot, b->stream, n, nullptr,
+                                 nullptr, block) == KLFT_OK
+                 ? cudaSuccess
+                 : cudaErrorLaunchFailure;
+    });
+    off = 0;
+    for (const auto &ch : b->chains) {
+      if (cudaMemcpyAsync(ch.lat->links, bak + off, ch.lat->link_bytes, cudaMemcpyDeviceToDevice, b->stream) !=
+          cudaSuccess)
+        return -1.f;
+      off += (ch.lat->link_bytes + 255) & ~(size_t)255;
+    }
+    if (cudaStreamSynchronize(b->stream) != cudaSuccess) return -1.f;
+    return ms;
+  };
+  b->sweep_block = tuned_param(key, 1, {32, 64, 128}, 128, time_fn, true);
+  b->s_tune.release();
   CK(cudaGetLastError());
   return KLFT_OK;
 }
@@ -523,7 +603,7 @@ klft_status klft_batch_destroy(klft_batch *b) {
     std::lock_guard<std::mutex> g(b->mtx);
     if (b->stream) cudaStreamSynchronize(b->stream);
     b->drop_graph();
-    for (klft::Scratch *s : {&b->s_nacc, &b->s_plaq, &b->s_labels, &b->s_ppart}) s->release();
+    for (klft::Scratch *s : {&b->s_nacc, &b->s_plaq, &b->s_labels, &b->s_ppart, &b->s_tune}) s->release();
     for (void *p : {(void *)b->d_slot, (void *)b->d_ctrs, (void *)b->d_c_of_label, (void *)b->d_c_of_rep,
                     (void *)b->d_A, (void *)b->d_part, (void *)b->d_label_of_rep, (void *)b->d_rep_of_label,
                     (void *)b->d_swap_acc})
@@ -613,6 +693,10 @@ klft_status klft_batch_run(klft_batch *b, int ncycles, int measure_plaquette, in
   for (auto &ch : b->chains) CK(cudaStreamSynchronize(ch.lat->stream));
   klft_status s = prepare(b, ncycles);
   if (s != KLFT_OK) return s;
+  if (b->dirty) {
+    s = tune_sweep_block(b);
+    if (s != KLFT_OK) return s;
+  }
   if (b->dirty || b->graph_measure != measure_plaquette) b->drop_graph();
   CK(cudaMemsetAsync(b->d_slot, 0, sizeof(uint32_t), b->stream));
   CK(cudaMemsetAsync(b->s_nacc.ptr, 0, (size_t)ncycles * n * sizeof(unsigned long long), b->stream));

@@ -81,8 +81,10 @@ struct StreamFork {
   const cudaEvent_t *join;  // one per side stream
   int nside;
 };
+// block: threads per CTA of the multi-chain launches (32, 64 or 128; results do not depend on it)
 klft_status enqueue_multi_sweep(const std::vector<SweepItem> &items, unsigned long long *nacc, const uint32_t *slot,
-                                cudaStream_t st, int acc_stride, int *nlaunch, const StreamFork *fork = nullptr);
+                                cudaStream_t st, int acc_stride, int *nlaunch, const StreamFork *fork = nullptr,
+                                int block = 128);
 // sweep counters += 1: a device array of counter pointers, or a host list
 cudaError_t launch_advance_many(uint32_t *const *d_ctrs, int n, cudaStream_t st);
 cudaError_t launch_advance_list(const std::vector<uint32_t *> &ctrs, cudaStream_t st, int *nlaunch);

@@ -85,3 +85,39 @@ def test_batch_ptbc_replicas_match_host_swaps():
     for r in range(nrep):
         np.testing.assert_array_equal(reps_b[r].download(), reps_s[r].download())
     b.close()
+
+
+def test_batch_tuning_changes_nothing(tmp_path):
+    """KLFT_TUNING's batch block-size search times candidates on the chains'
+    own links (backed up and restored) and caches a key per batch composition;
+    the chains end exactly where an untuned batch takes them."""
+    import klft_b200
+    from klft_b200._lib import lib
+    cache = str(tmp_path / "tune.txt")
+    runs = {}
+    try:
+        for tuned in (True, False):
+            lib().klft_tuner_clear()
+            lib().klft_tuner_configure(int(tuned), 0)
+            b = klft_b200.Batch()
+            fields = []
+            for k, (L, nc, prec, beta, delta, nh, prop, eps) in enumerate(CHAINS):
+                g = make(L, nc, prec, 700 + k, k)
+                b.add(g, beta, delta, nh, prop, eps)
+                fields.append(g)
+            acc, plaq, _, _ = b.run(3, True, True)
+            acc2, _, _, _ = b.run(2, False, False)
+            if tuned:
+                assert lib().klft_tuner_write_cache(cache.encode()) == 0
+            runs[tuned] = (acc, plaq, acc2, [g.download() for g in fields], [g.counters() for g in fields])
+            b.close()
+    finally:
+        lib().klft_tuner_configure(0, 0)
+        lib().klft_tuner_clear()
+    assert "sweep_Metropolis_batch_" in open(cache).read()
+    a, u = runs[True], runs[False]
+    for x, y in zip(a[:3], u[:3]):
+        np.testing.assert_array_equal(x, y)
+    for x, y in zip(a[3], u[3]):
+        np.testing.assert_array_equal(x, y)
+    assert a[4] == u[4]
