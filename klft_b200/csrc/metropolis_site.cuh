@@ -149,17 +149,17 @@ KLFT_D int site_update_ref(const Links<NC, T> &U, const Geom &g, const Site &x, 
   return nacc;
 }
 
-// SU(3) exp(i eps H) proposals U' = X U at fixed stream positions.
-// Re Tr(X U S) = Re Tr(X M) with M = U S carried in registers; an accepted
-// proposal updates U <- X U and M <- X M (no reprojection between hits: X is
-// unitary to round-off) and the link is reunitarised once after its hits.  The link waits in shared memory, one
-// structure-of-arrays slot per thread, leaving registers to the proposal; the
-// staple is not needed after M is formed.
+// SU(3) exp(i eps H) proposals U' = X U at fixed stream positions.  The
+// accepted proposals of a link accumulate into A = X_k ... X_1, so the current
+// link is A U0 and, with M0 = U0 S formed once, a hit's action change needs
+// Re Tr(X A U0 S) = Re Tr((X A) M0): one product X A per hit, which also is the
+// new A when the hit is accepted (every warp takes the accept branch on almost
+// every hit, so this halves the products per hit against carrying U and U S).
+// The link is rebuilt as A U0 and reunitarised once after its hits.  The Markov
+// chain is the one of U <- X U per accepted hit; only the rounding differs.
 template <int ND, typename T, bool DF>
 KLFT_D int site_update_exp(const Links<3, T> &U, const Geom &g, const Site &x, const MetroArgs &a, uint32_t sweep,
                            const Defect &df) {
-  __shared__ cx<T> s_U[9][128];
-  const int tid = threadIdx.x;
   int nacc = 0;
   const ExpHitStream hs{(uint32_t)a.seed, (uint32_t)(a.seed >> 32) ^ (uint32_t)a.chain, site_lex(g, x), sweep};
   const long long lx = site_lin(g, x);
@@ -169,16 +169,12 @@ KLFT_D int site_update_exp(const Links<3, T> &U, const Geom &g, const Site &x, c
   for (int mu = 0; mu < ND; ++mu) {
     if (open_link(g, x, mu)) continue;
     const uint32_t h0 = (uint32_t)(mu * a.nhits);
-    Mat<3, T> M;
-    {
-      const Mat<3, T> Uo = U.load(lx, mu);
-      const Mat<3, T> S = staple<3, ND, T, DF>(U, g, x, mu, df);
-#pragma unroll
-      for (int k = 0; k < 9; ++k) s_U[k][tid] = Uo.e[k / 3][k % 3];
-      M = mul(Uo, S);
-    }
+    // M0 = U0 S stays fixed; A is the product of the accepted X, so the current
+    // link is A U0 and Re Tr(X A U0 S) = Re Tr((X A) M0): one product X A per hit
+    const Mat<3, T> M0 = mul(U.load(lx, mu), staple<3, ND, T, DF>(U, g, x, mu, df));
+    Mat<3, T> A = mident<3, T>();
     const bool dlink = DF && df.active && in_defect(g, df, x, mu);
-    T trO = retr_diag(M);
+    T trO = retr_diag(M0);
     bool changed = false;
     uint32_t aw[4];
     // the Philox words of hit h + 1 are drawn while hit h is evaluated
@@ -196,29 +192,19 @@ KLFT_D int site_update_exp(const Links<3, T> &U, const Geom &g, const Site &x, c
         hs.block(2 * (h + 1), wn);
         hs.block(2 * (h + 1) + 1, wn + 4);
       }
-      const Mat<3, T> rr = exp_proposal_w<T>(w, half_eps);
-      T dS = -bnc * (retr_mul(rr, M) - trO);
+      const Mat<3, T> Y = mul(exp_proposal_w<T>(w, half_eps), A);
+      const T tY = retr_mul(Y, M0);
+      T dS = -bnc * (tY - trO);
       if (dlink) dS *= (T)defect_c(df);
       const bool accept = dS < T(0) || accept_word(aw, h) < (double)exp(-dS);
       if (accept) {
-        Mat<3, T> Uo;
-#pragma unroll
-        for (int k = 0; k < 9; ++k) Uo.e[k / 3][k % 3] = s_U[k][tid];
-        Uo = mul(rr, Uo);
-#pragma unroll
-        for (int k = 0; k < 9; ++k) s_U[k][tid] = Uo.e[k / 3][k % 3];
-        M = mul(rr, M);
-        trO = retr_diag(M);
+        A = Y;
+        trO = tY;
         ++nacc;
         changed = true;
       }
     }
-    if (changed) {
-      Mat<3, T> Uo;
-#pragma unroll
-      for (int k = 0; k < 9; ++k) Uo.e[k / 3][k % 3] = s_U[k][tid];
-      U.store(lx, mu, restore(Uo));
-    }
+    if (changed) U.store(lx, mu, restore(mul(A, U.load(lx, mu))));
   }
   return nacc;
 }

@@ -46,7 +46,11 @@ def test_gpu_ensemble_matches_reference_code(refshim, nc, beta, delta, start):
 
 def test_mixed_form_ensemble_matches_fp64():
     """SU(3) 8^4, beta 6, exp(i eps H) proposals: the mixed form and the FP64 form
-    sample the same distribution (independent chains)."""
+    sample the same distribution (independent chains).  The seeds are fixed, so
+    the outcome is deterministic, but any rounding-level change in either form
+    draws new chains: with four comparisons, 3 sigma keeps the chance of a false
+    alarm per redraw near 1 % (at 2 sigma it is ~17 %).  The precise check is
+    the batched one below and `python -m klft_b200.ensemble`."""
     L = [8, 8, 8, 8]
     pairs = [(1, 1), (2, 2), (2, 4)]
     res = {}
@@ -57,6 +61,23 @@ def test_mixed_form_ensemble_matches_fp64():
         _, plaq, w, _ = g.run_cycles(6.0, 0.0, 10, 1500, "exp", 0.25, True, pairs)
         res[prec] = (plaq, w)
         assert g.unitarity() < (1e-5 if prec == "mixed" else 1e-12)
-    assert_agree("SU(3) plaquette mixed vs fp64", res["mixed"][0], res["fp64"][0])
+    assert_agree("SU(3) plaquette mixed vs fp64", res["mixed"][0], res["fp64"][0], zmax=3.0)
     for k, p in enumerate(pairs):
-        assert_agree(f"SU(3) W{p} mixed vs fp64", res["mixed"][1][:, k], res["fp64"][1][:, k])
+        assert_agree(f"SU(3) W{p} mixed vs fp64", res["mixed"][1][:, k], res["fp64"][1][:, k], zmax=3.0)
+
+
+def test_mixed_form_batched_ensemble_matches_fp64():
+    """64 independent SU(3) 8^4 chains per form in one batch; each chain's mean
+    plaquette over 1000 cycles (after 300) is one sample, so the error of the
+    ensemble mean needs no autocorrelation model: the two forms agree within
+    2 sigma at errors of ~7e-5."""
+    from klft_b200.ensemble import run_form, summary
+    out = {}
+    for prec in ("mixed", "fp64"):
+        means, _ = run_form(prec, [8, 8, 8, 8], 3, 6.0, 10, "exp", 0.25, 0.0, 64, 300, 1000, 4100)
+        out[prec] = summary(means)
+    (m1, e1), (m2, e2) = out["mixed"], out["fp64"]
+    z = (m1 - m2) / np.hypot(e1, e2)
+    print(f"batched plaquette mixed vs fp64: {m1:.6f} +- {e1:.6f} vs {m2:.6f} +- {e2:.6f}  z = {z:+.2f}")
+    assert e1 < 2e-4 and e2 < 2e-4
+    assert abs(z) < 2.0
