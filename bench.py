@@ -265,12 +265,15 @@ TRAFFIC_SOURCE = "profiles/metropolis_exp_su3_32x4_mixed.md"
 
 def sweep_flops_per_link_update(nhits: int, acceptance: float) -> float:
     """Algorithmic flops of one SU(3) exp(i eps H) link update (6 per complex
-    multiply, 2 per complex add, 198 per 3x3 product): staple 2466, M = U S 198,
+    multiply, 2 per complex add, 198 per 3x3 product): staple 2466, M0 = U0 S 198,
     per hit the proposal (8 Box-Muller normals 32, Gell-Mann sum 16, Q^2 132,
-    c0/c1 30, 12-term coefficient series 108, X = f0 + f1 Q + f2 Q^2 126) + Re Tr(X M)
-    36 + acceptance x (X U, X M) 396, and one reunitarisation (~100)."""
+    c0/c1 30, 12-term coefficient series 108, X = f0 + f1 Q + f2 Q^2 126), the
+    product X A with the accepted proposals 198 and Re Tr(X A M0) 36; then the
+    link A U0 198 and one reunitarisation (~100).  The accept rate no longer
+    enters: the one product per hit is also the accepted A."""
+    del acceptance
     proposal = 32 + 16 + 132 + 30 + 108 + 126
-    return 2466 + 198 + nhits * (proposal + 36 + acceptance * 396) + 100
+    return 2466 + 198 + nhits * (proposal + 198 + 36) + 198 + 100
 
 
 def mixed_errors(g, L):
