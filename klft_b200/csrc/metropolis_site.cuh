@@ -192,7 +192,8 @@ KLFT_D int site_update_exp(const Links<3, T> &U, const Geom &g, const Site &x, c
         hs.block(2 * (h + 1), wn);
         hs.block(2 * (h + 1) + 1, wn + 4);
       }
-      const Mat<3, T> Y = mul(exp_proposal_w<T>(w, half_eps), A);
+      const Mat<3, T> X = exp_proposal_w<T>(w, half_eps);
+      const Mat<3, T> Y = hit == 0 ? X : mul(X, A);  // A is the identity before the first hit
       const T tY = retr_mul(Y, M0);
       T dS = -bnc * (tY - trO);
       if (dlink) dS *= (T)defect_c(df);
