@@ -125,6 +125,37 @@ KLFT_D int site_update_ref(const Links<NC, T> &U, const Geom &g, const Site &x, 
     if (open_link(g, x, mu)) continue;
     const Mat<NC, T> S = staple<NC, ND, T, DF>(U, g, x, mu, df);
     const bool dlink = DF && df.active && in_defect(g, df, x, mu);
+    if constexpr (NC <= 2) {
+      // U(1), SU(2): accepted proposals accumulate into A = r_1 ... r_k, so the
+      // current link is U0 A and Re Tr(U0 A r S) = Re Tr((A r) M0), M0 = S U0: one
+      // product A r per hit, which is also the new A on acceptance (warps take the
+      // accept branch on almost every hit).  The link is rebuilt as U0 A and
+      // reunitarised once; the chain is the one of U <- restore(U r) per accepted
+      // hit, with rounding-level differences.
+      const Mat<NC, T> U0 = U.load(lx, mu);
+      const Mat<NC, T> M0 = mul(S, U0);
+      Mat<NC, T> A = mident<NC, T>();
+      T trO = retr_diag(M0);
+      bool changed = false;
+#pragma unroll 1
+      for (int hit = 0; hit < a.nhits; ++hit) {
+        const Mat<NC, T> rr = propose<T>(rng, (const Mat<NC, T> *)nullptr, a.delta, PROPOSAL_REFERENCE, 0.0);
+        const Mat<NC, T> Y = hit == 0 ? rr : mul(A, rr);
+        const T tY = retr_mul(Y, M0);
+        T dS = -bnc * (tY - trO);
+        if (dlink) dS *= (T)defect_c(df);
+        bool accept = dS < T(0);
+        if (!accept) accept = rng.next() < (double)exp(-dS);
+        if (accept) {
+          A = Y;
+          trO = tY;
+          ++nacc;
+          changed = true;
+        }
+      }
+      if (changed) U.store(lx, mu, restore(mul(U0, A)));
+      continue;
+    }
     Mat<NC, T> Uo = U.load(lx, mu);
     Mat<NC, T> M = mul(S, Uo);
     T trO = retr_diag(M);
