@@ -9,9 +9,12 @@
 // dS = -(beta/Nc) Re Tr[(U' - U) S], and an accepted link is stored
 // reunitarised (restoreSUN).
 //
-// Per-hit cost is cut by carrying M = S U: Re Tr(U r S) = Re Tr(r M) needs only
-// the diagonal of r M (36 flops for SU(3)) instead of the product U r; U r and M
-// are rebuilt only on acceptance.
+// Per-hit cost: with M = S U, Re Tr(U r S) = Re Tr(r M) needs only the diagonal
+// of r M.  SU(3) reference proposals (a few per cent accepted) rebuild U r and M
+// on acceptance; U(1)/SU(2) and the exp(i eps H) proposals, accepted on
+// ~30-70 % of hits (so every warp runs the accept branch on nearly every hit),
+// accumulate the accepted proposals into one matrix A instead and need one
+// product per hit (see site_update_ref and site_update_exp).
 //
 // Random numbers: the reference proposals (U(1), SU(2), the SU(3)
 // Gram-Schmidt generator) consume the site's sequential Philox stream in the
