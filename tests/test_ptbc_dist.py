@@ -49,7 +49,10 @@ def test_swap_sums_reject_bad_labels():
         klft_b200.ptbc_swap_sums(sums(0), np.linspace(1, 0, NREP), [0, 0, 1, 2, 3], SEED, 0)
 
 
-def _rank(rank, world, port, q, dup):
+SPLITS = {"even": SPLIT, "empty_rank": {0: [0, 1, 2, 3, 4], 1: []}}
+
+
+def _rank(rank, world, port, q, dup, split_name="even"):
     os.environ.update({"MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port)})
     sys.path.insert(0, ROOT)
     import datetime
@@ -60,7 +63,7 @@ def _rank(rank, world, port, q, dup):
     from klft_b200.ptbc_dist import gather_defect_sums
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
     try:
-        ids = [0] if dup else SPLIT[rank]
+        ids = [0] if dup else SPLITS[split_name][rank]
         c = np.linspace(1.0, 0.0, NREP)
         lab = np.arange(NREP)
         seq = []
@@ -76,11 +79,11 @@ def _rank(rank, world, port, q, dup):
         dist.destroy_process_group()
 
 
-def _run(dup):
+def _run(dup, split_name="even"):
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = free_port()
-    ps = [ctx.Process(target=_rank, args=(r, 2, port, q, dup)) for r in range(2)]
+    ps = [ctx.Process(target=_rank, args=(r, 2, port, q, dup, split_name)) for r in range(2)]
     for p in ps:
         p.start()
     for p in ps:
@@ -89,9 +92,10 @@ def _run(dup):
     return sorted(q.get(timeout=10) for _ in range(2))
 
 
-def test_gathered_swaps_agree_on_every_rank():
+@pytest.mark.parametrize("split_name", ["even", "empty_rank"])
+def test_gathered_swaps_agree_on_every_rank(split_name):
     import klft_b200
-    got = _run(False)
+    got = _run(False, split_name)
     assert [g[1] for g in got] == ["ok", "ok"]
     assert got[0][2] == got[1][2]
     c = np.linspace(1.0, 0.0, NREP)
