@@ -507,6 +507,10 @@ static double metropolis_sweep(const Field<NC> &F, double beta, double delta, in
   for (int i = 0; i < (1 << nd); ++i) {
     int bit[4] = {0, 0, 0, 0};
     for (int k = 0; k < nd; ++k) bit[nd - 1 - k] = (i >> k) & 1;  // IndexHelper.hpp:84-93
+    // sites of one parity class share no staple link and each reads its own
+    // random stream, so the class loop may run on several threads with the
+    // same result (the reference runs it as one parallel_for)
+#pragma omp parallel for schedule(static) reduction(+ : nacc) if (Vh >= 4096)
     for (long h = 0; h < Vh; ++h) {
       int x[4] = {0, 0, 0, 0};
       long t = h;

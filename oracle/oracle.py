@@ -15,8 +15,10 @@ Arrays use the host interchange layout: complex128 of shape
 from __future__ import annotations
 
 import ctypes as C
+import glob
 import os
 import subprocess
+import sys
 
 import numpy as np
 
@@ -34,11 +36,31 @@ _up = C.POINTER(C.c_uint32)
 
 
 def build(force: bool = False) -> None:
-    """Compile liboracle.so (and libklft_ref.so when the reference tree exists)."""
-    if force or not os.path.exists(ORACLE_SO):
+    """Compile liboracle.so, and libklft_ref.so from the klft source tree that
+    the environment variable KLFT_REF_DIR names.
+
+    Without KLFT_REF_DIR an existing libklft_ref.so is kept as built; when there
+    is none, the reference-code checks are skipped and this says so on stderr.
+    """
+    if force or _stale(ORACLE_SO, [os.path.join(HERE, "oracle.cpp")]):
         subprocess.run(["make", "-C", HERE, "all"], check=True, capture_output=True)
-    if os.path.isdir("/root/reference/include") and (force or not os.path.exists(REF_SO)):
-        subprocess.run(["make", "-C", HERE, "ref"], check=True, capture_output=True)
+    ref_dir = os.environ.get("KLFT_REF_DIR", "")
+    if ref_dir:
+        if not os.path.isdir(os.path.join(ref_dir, "include")):
+            raise FileNotFoundError(f"KLFT_REF_DIR={ref_dir} has no include/ directory")
+        deps = [os.path.join(HERE, "ref_harness.cpp")] + glob.glob(os.path.join(HERE, "ref_shim", "*.hpp"))
+        if force or _stale(REF_SO, deps):
+            subprocess.run(["make", "-C", HERE, "ref", "KLFT_REF_DIR=" + ref_dir], check=True, capture_output=True)
+    elif not os.path.exists(REF_SO):
+        sys.stderr.write("oracle: KLFT_REF_DIR is not set and oracle/_ref/libklft_ref.so does not exist; "
+                         "the checks against klft's own code are skipped\n")
+
+
+def _stale(target: str, deps) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
 
 
 def _d(a):
