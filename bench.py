@@ -345,26 +345,66 @@ def bench_batched_ptbc(cycles: int, warmup: int = 3):
     return out
 
 
-def bench_hmc(ntraj: int):
-    """SU(2) 24^4 HMC, beta = 2.3, tau = 1, 20 leapfrog steps, hot start: mixed vs FP64."""
+def bench_hmc(ntraj: int, cpu: bool = True):
+    """SU(2) 24^4 HMC, beta = 2.3, tau = 1, 20 steps, hot start, mixed vs FP64.
+
+    as_given: klft's Pauli generators and the 20-step leapfrog, the workload as
+    stated; its effective step is twice that of the t_a/2 normalisation and at
+    this volume it accepts almost nothing.  accepting: t_a/2 generators and the
+    20-step Omelyan integrator from the same kind of hot start, thermalised by
+    HMC itself (100 trajectories), then ntraj measured trajectories with the
+    acceptance, <exp(-dH)> with its standard error, <dH> and the mean
+    plaquette.  cpu_oracle: one as-given trajectory of the FP64 oracle on the
+    host threads (OpenMP force and updates)."""
     import klft_b200
-    out = {"workload": f"SU(2) 4D 24^4 HMC beta=2.3 tau=1 20 leapfrog steps, {ntraj} trajectories from a "
-                       "hot start (seed 4242)"}
-    for prec in ("mixed", "fp64"):
-        g = klft_b200.GaugeField([24] * 4, 2, prec, "hot", 4242)
-        g.set_stream(4242, 0)
-        g.hmc(2.3, 1.0, 20, 2, "leapfrog")  # warm-up (2 trajectories, same stream continues)
-        t0 = time.perf_counter()
-        dH, acc = g.hmc(2.3, 1.0, 20, ntraj, "leapfrog")
-        dt = time.perf_counter() - t0
-        out[prec] = {"trajectories_per_s": ntraj / dt, "ms_per_trajectory": dt * 1e3 / ntraj,
-                     "acceptance": float(np.mean(acc != 0)),
-                     "acceptance_last_half": float(np.mean(acc[ntraj // 2:] != 0)),
-                     "mean_exp_mdH_last_half": float(np.mean(np.exp(np.minimum(-dH[ntraj // 2:], 700.0)))),
-                     "mean_dH_last_half": float(np.mean(dH[ntraj // 2:])),
-                     "plaquette": g.plaquette(), "unitarity": g.unitarity()}
+    out = {"workload": f"SU(2) 4D 24^4 HMC beta=2.3 tau=1 20 steps, {ntraj} trajectories from a hot start"}
+
+    def run(prec, generators, integrator, ntherm, seed):
+        g = klft_b200.GaugeField([24] * 4, 2, prec, "hot", seed)
+        g.set_stream(seed, 0)
+        g.set_hmc_generators(generators)
+        g.hmc(2.3, 1.0, 20, max(ntherm, 2), integrator)  # warm-up / thermalisation, same stream continues
+        dHs, accs, plaqs = [], [], []
+        t_dev = 0.0
+        nblk = 5
+        for b in range(nblk):
+            n = ntraj // nblk + (1 if b < ntraj % nblk else 0)
+            t0 = time.perf_counter()
+            dH, acc = g.hmc(2.3, 1.0, 20, n, integrator)
+            t_dev += time.perf_counter() - t0
+            dHs.append(dH)
+            accs.append(acc)
+            plaqs.append(g.plaquette())
+        dH = np.concatenate(dHs)
+        acc = np.concatenate(accs)
+        e = np.exp(np.minimum(-dH, 700.0))
+        r = {"trajectories_per_s": ntraj / t_dev, "ms_per_trajectory": t_dev * 1e3 / ntraj,
+             "acceptance": float(np.mean(acc != 0)),
+             "acceptance_last_half": float(np.mean(acc[ntraj // 2:] != 0)),
+             "mean_exp_mdH": float(np.mean(e)), "mean_exp_mdH_err": float(np.std(e, ddof=1) / np.sqrt(len(e))),
+             "mean_dH": float(np.mean(dH)), "mean_plaquette": float(np.mean(plaqs)),
+             "unitarity": g.unitarity()}
         g.close()
-    out["speedup_mixed_vs_fp64"] = out["mixed"]["trajectories_per_s"] / out["fp64"]["trajectories_per_s"]
+        return r
+
+    out["as_given"] = {"generators": "reference (Pauli)", "integrator": "leapfrog, 20 steps"}
+    out["accepting"] = {"generators": "half (t_a/2)", "integrator": "omelyan, 20 steps", "thermalisation": 100}
+    for prec in ("mixed", "fp64"):
+        out["as_given"][prec] = run(prec, "reference", "leapfrog", 2, 4242)
+        out["accepting"][prec] = run(prec, "half", "omelyan", 100, 4343)
+    for k in ("as_given", "accepting"):
+        out[k]["speedup_mixed_vs_fp64"] = (out[k]["mixed"]["trajectories_per_s"] /
+                                           out[k]["fp64"]["trajectories_per_s"])
+    if cpu:
+        from oracle.oracle import INTEGRATOR_LEAPFROG, Lat, Oracle
+        o = Oracle()
+        lat = Lat(2, [24] * 4)
+        U = o.init(lat, True, 4242)
+        t0 = time.perf_counter()
+        o.hmc(lat, U, 2.3, 1.0, 20, INTEGRATOR_LEAPFROG, 4242, 0, 0, 1)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"trajectories_per_s": 1.0 / dt, "kind": "port", "cores": os.cpu_count(),
+                             "sample": "1 as-given FP64 trajectory of the oracle (SU(2) 24^4, 20 leapfrog steps)"}
     return out
 
 
@@ -481,7 +521,7 @@ def run_ours(a, dist: Dist):
                                 "note": "V*Nd(Nd-1)/2 plaquettes per GaugePlaquette, device time"}
     if dist.world == 1 and not a.no_extras:
         for key, fn in (("batched_ptbc", lambda: bench_batched_ptbc(a.batch_cycles)),
-                        ("hmc", lambda: bench_hmc(a.hmc_traj)),
+                        ("hmc", lambda: bench_hmc(a.hmc_traj, not a.no_cpu_baseline)),
                         ("serving", lambda: bench_serving(a.serve_jobs, a.serve_rate))):
             try:
                 line[key] = fn()

@@ -67,6 +67,7 @@ struct HMCParams {
   std::string outfilename;
   int integrator = KLFT_INTEGRATOR_REFERENCE_LEAPFROG;
   int precision = KLFT_PRECISION_FP64;
+  int generators = KLFT_GENERATORS_REFERENCE;  // klft_hmc_set_generators
 };
 
 // InputParser.hpp:33-125: false (and a message) when the block is missing or malformed

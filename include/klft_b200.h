@@ -143,6 +143,18 @@ klft_status klft_gauge_force(klft_lattice *lat, double beta, double *host_force)
  * monomial energy -(beta/Nc) sum_P Re Tr P (GaugeMonomial.hpp:19-25), FP64. */
 klft_status klft_hmc_energies(klft_lattice *lat, double beta, double *kinetic, double *gauge_action);
 
+/* Normalisation of the HMC generators of a lattice.  REFERENCE (the default)
+ * is klft's: t_a = Pauli matrices for SU(2) (AdjointGroup.hpp:98-105), the
+ * Gell-Mann matrices for SU(3), U(1) e^{i p}.  HALF uses t_a / 2 (the common
+ * normalisation, Tr t_a t_b = delta_ab / 2): U <- exp(i dt sum_a p_a t_a / 2) U
+ * and F_a = (beta/Nc) Im Tr(t_a U S) / 2, with the same N(0,1) momenta and
+ * kinetic energy.  Its leapfrog/Omelyan step of length dt is the reference
+ * step of length dt/2, so HALF with (tau, n_steps) is the REFERENCE
+ * trajectory with (tau/2, n_steps); klft_gauge_force returns the HALF force.
+ * Server jobs use REFERENCE. */
+typedef enum { KLFT_GENERATORS_REFERENCE = 0, KLFT_GENERATORS_HALF = 1 } klft_generators;
+klft_status klft_hmc_set_generators(klft_lattice *lat, int generators);
+
 /* ---------------------------------------------------------------- PTBC
  * PTBCGaugeField set_defect / shift_defect (PTBCGaugeField.hpp:187-206): links
  * mu = 0 at x0 = 0 whose spatial coordinates lie in pos + [0, len) (periodic)
@@ -320,7 +332,11 @@ klft_status klft_server_inject_fault(klft_server *s, int what);
  * of handle scratch.  nsweeps above that limit is rejected with KLFT_EINVAL.
  * The lattice's device must be current.  The first call on a device looks up
  * the array's device address (cudaGetSymbolAddress); make that first call
- * before any stream capture.  All calls on a device share the array: each call
+ * before any stream capture.  That first call (like the first launch of any
+ * kernel) may also make the driver load the library's kernels, which can
+ * allocate driver memory once: a warm-up call after creating the lattice makes
+ * every later call allocation-free.  The tuner is not started from here; a
+ * launch shape it already chose is used.  All calls on a device share the array: each call
  * clears the counters it uses, and because calls whose GPU work overlapped
  * would race on them, a call holds a per-device lock until its stream is done. */
 #define KLFT_NOALLOC_MAX_SWEEPS 1024
@@ -331,6 +347,17 @@ klft_status klft_metropolis_sweeps_noalloc(klft_lattice *lat, double beta, doubl
  * (dtype 0: FP64, 1: FP32) of the current device in TFLOP/s, the roofline
  * denominator of this library's SU(N) kernels. */
 klft_status klft_peak_flops(int dtype, double *tflops);
+
+/* Diagnostic with no reference counterpart: the error of the mixed form's
+ * Metropolis action change on one configuration.  For every link of an FP64
+ * SU(3) lattice and each of its nhits exp(i eps H) proposals of the current
+ * sweep's stream, dS is formed twice with the same proposal: in FP64 from the
+ * FP64 links, and in FP32 from the links as the mixed form stores them (two FP32
+ * rows).  out[0] hits, out[1] mean and out[2] rms of d = dS32 - dS64, out[3]
+ * max |d|, out[4] the slope sum(dS64 d) / sum(dS64^2) (a relative error of the
+ * action change, i.e. of beta), out[5] the fraction of hits whose accept
+ * decision differs with the hit's uniform.  The links are not changed. */
+klft_status klft_exp_proposal_dS_error(klft_lattice *lat, double beta, double eps, int nhits, double *out);
 
 #ifdef __cplusplus
 }

@@ -28,6 +28,7 @@ PRECISION = {"fp64": 0, "mixed": 1}
 START = {"cold": 0, "hot": 1}
 PROPOSAL = {"reference": 0, "exp": 1}
 INTEGRATOR = {"reference": 0, "leapfrog": 1, "omelyan": 2}
+GENERATORS = {"reference": 0, "half": 1}
 
 __all__ = [
     "GaugeField", "MetropolisParams", "GaugeObservableParams", "KlftError", "sweep_Metropolis",
@@ -228,6 +229,12 @@ class GaugeField:
         k, s = C.c_double(), C.c_double()
         check(lib().klft_hmc_energies(self._h, beta, C.byref(k), C.byref(s)))
         return k.value, s.value
+
+    def set_hmc_generators(self, generators: str) -> None:
+        """"reference" (klft's Pauli / Gell-Mann generators, the default) or
+        "half" (t_a / 2: a trajectory of length tau equals the reference one of
+        length tau / 2)."""
+        check(lib().klft_hmc_set_generators(self._h, GENERATORS[generators]))
 
     # -- PTBC
     def set_open_boundary(self, mu: int) -> None:

@@ -73,6 +73,7 @@ SIGNATURES = {
     "klft_run_cycles": (C.c_int, [_vp, C.c_double, C.c_double, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, _ip,
                                   C.c_int, _dp, _dp, _dp, _dp]),
     "klft_peak_flops": (C.c_int, [C.c_int, _dp]),
+    "klft_exp_proposal_dS_error": (C.c_int, [_vp, C.c_double, C.c_double, C.c_int, _dp]),
     "klft_hmc_trajectories": (C.c_int, [_vp, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, _dp, _ip]),
     "klft_hmc_integrate": (C.c_int, [_vp, C.c_double, C.c_double, C.c_int, C.c_int]),
     "klft_hmc_refresh_momenta": (C.c_int, [_vp]),
@@ -80,6 +81,7 @@ SIGNATURES = {
     "klft_hmc_get_momenta": (C.c_int, [_vp, _dp]),
     "klft_gauge_force": (C.c_int, [_vp, C.c_double, _dp]),
     "klft_hmc_energies": (C.c_int, [_vp, C.c_double, _dp, _dp]),
+    "klft_hmc_set_generators": (C.c_int, [_vp, C.c_int]),
     "klft_lattice_set_defect": (C.c_int, [_vp, C.c_int, _ip, C.c_double]),
     "klft_batch_create": (C.c_int, [C.POINTER(_vp)]),
     "klft_batch_destroy": (C.c_int, [_vp]),

@@ -110,7 +110,7 @@ klft_status klft::lattice_sync(klft_lattice *lat) {
 
 // Proposal arguments: the reference SU(3) generator needs delta > 0 (its
 // rejection loops draw from [0, delta) until the norm is nonzero).
-static klft_status check_proposal(const klft_lattice *lat, double delta, int proposal, double eps, const char *who) {
+klft_status klft::check_proposal(const klft_lattice *lat, double delta, int proposal, double eps, const char *who) {
   if (proposal != KLFT_PROPOSAL_REFERENCE && proposal != KLFT_PROPOSAL_EXP)
     return fail(KLFT_EINVAL, "%s: unknown proposal %d", who, proposal);
   if (!(delta == delta) || !(eps == eps)) return fail(KLFT_EINVAL, "%s: NaN step size", who);

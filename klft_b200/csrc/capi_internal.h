@@ -37,6 +37,12 @@ klft_status cuda_fail(cudaError_t e, const char *what);
 
 }  // namespace klft
 
+namespace klft {
+// The proposal arguments every sweep entry point accepts (who names the caller
+// in the error message).
+klft_status check_proposal(const klft_lattice *lat, double delta, int proposal, double eps, const char *who);
+}  // namespace klft
+
 struct klft_lattice {
   int nc = 0;
   int precision = 0;
@@ -50,6 +56,7 @@ struct klft_lattice {
   double *h_results = nullptr;     // pinned, KLFT_RESULT_SLOTS doubles
   klft::Scratch s_part, s_out, s_aux, s_stage, s_wl, s_hmc, s_gf, s_tab, s_tune;
   int hmc_cap = 0;  // trajectories the HMC buffers in s_hmc are laid out for
+  int hmc_generators = KLFT_GENERATORS_REFERENCE;
   klft::Defect defect{0, 1, {0, 0, 0}, 1.0, nullptr};
   std::mutex mtx;
   int dtype() const { return precision == KLFT_PRECISION_FP64 ? 0 : 1; }

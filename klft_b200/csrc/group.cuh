@@ -1,7 +1,9 @@
-// group.cuh -- group-specific device math: Metropolis proposals, the SU(3)
-// exponential, Haar-random links, and the Lie-algebra maps used by HMC.
+// group.cuh -- group-specific device math: Metropolis proposals, Haar-random
+// links, and the Lie-algebra maps used by HMC (the SU(3) exponential is in
+// expprop.cuh).
 #pragma once
 #include "common.cuh"
+#include "expprop.cuh"
 
 namespace klft {
 
@@ -9,124 +11,6 @@ constexpr double KPI = 3.141592653589793;
 constexpr double K2PI = 6.283185307179586;
 
 enum Proposal : int { PROPOSAL_REFERENCE = 0, PROPOSAL_EXP = 1 };
-
-// ------------------------------------------------------------------ SU(3) exponential
-// exp(iQ) for hermitian traceless 3x3 Q in the Cayley-Hamilton basis
-// (1, Q, Q^2) (cf. Morningstar & Peardon, Phys. Rev. D 69 (2004) 054501).
-// Q^2 of a hermitian Q: the upper triangle, mirrored.
-template <typename T> KLFT_D Mat<3, T> herm_square(const Mat<3, T> &Q) {
-  Mat<3, T> Q2;
-#pragma unroll
-  for (int i = 0; i < 3; ++i) {
-    T d = T(0);
-#pragma unroll
-    for (int k = 0; k < 3; ++k) d += Q.e[i][k].re * Q.e[i][k].re + Q.e[i][k].im * Q.e[i][k].im;
-    Q2.e[i][i] = mk<T>(d, T(0));
-#pragma unroll
-    for (int j = i + 1; j < 3; ++j) {
-      cx<T> s = Q.e[i][0] * Q.e[0][j];
-#pragma unroll
-      for (int k = 1; k < 3; ++k) s += Q.e[i][k] * Q.e[k][j];
-      Q2.e[i][j] = s;
-      Q2.e[j][i] = conj(s);
-    }
-  }
-  return Q2;
-}
-
-// exp(iQ) = f0 + f1 Q + f2 Q^2 for hermitian traceless 3x3 Q, with the f_j
-// summed in coefficient space.  Cayley-Hamilton gives Q^3 = c1 Q + c0 with
-// c1 = Tr Q^2 / 2 and c0 = det Q (real), so every power Q^n = a_n + b_n Q + d_n Q^2
-// with the real recurrence (a, b, d)_{n+1} = (d c0, a + d c1, b), and
-// f = sum_n i^n/n! (a_n, b_n, d_n).  Arguments with c1 > 3/4 (an eigenvalue
-// possibly above 1: |lambda|^2 <= 4 c1 / 3) are scaled by 2^-s and the result
-// squared s times, also in coefficient space:
-//   (f0 + f1 Q + f2 Q^2)^2 = (f0^2 + 2 f1 f2 c0) + (2 f0 f1 + 2 f1 f2 c1 + f2^2 c0) Q
-//                          + (f1^2 + 2 f0 f2 + f2^2 c1) Q^2.
-// Terms: 12 in FP32 and 19 in FP64 (|lambda| <= 1: 1/12! < 3e-9, 1/19! < 1e-17).
-template <typename T> struct ExpTerms { static constexpr int n = 12; };
-template <> struct ExpTerms<double> { static constexpr int n = 19; };
-
-template <typename T> KLFT_D Mat<3, T> expi_su3(const Mat<3, T> &Q) {
-  const Mat<3, T> Q2 = herm_square(Q);
-  T c1 = T(0.5) * (Q2.e[0][0].re + Q2.e[1][1].re + Q2.e[2][2].re);
-  // c0 = det Q, real for hermitian Q
-  T c0 = Q.e[0][0].re * (Q.e[1][1].re * Q.e[2][2].re - (Q.e[1][2].re * Q.e[1][2].re + Q.e[1][2].im * Q.e[1][2].im)) -
-         Q.e[1][1].re * (Q.e[0][2].re * Q.e[0][2].re + Q.e[0][2].im * Q.e[0][2].im) -
-         Q.e[2][2].re * (Q.e[0][1].re * Q.e[0][1].re + Q.e[0][1].im * Q.e[0][1].im) +
-         T(2) * (Q.e[0][1] * Q.e[1][2] * Q.e[2][0]).re;
-  int sq = 0;
-  T scale = T(1);
-  while (c1 > T(0.75) && sq < 64) {  // halve Q: c1 / 4, c0 / 8
-    c1 *= T(0.25);
-    c0 *= T(0.125);
-    scale *= T(0.5);
-    ++sq;
-  }
-  // Taylor sum of exp(i Q'), Q' = scale Q, in the basis (1, Q', Q'^2)
-  T a = T(1), b = T(0), d = T(0), fact = T(1);
-  cx<T> f0 = mk<T>(T(1), T(0)), f1 = mk<T>(T(0), T(0)), f2 = mk<T>(T(0), T(0));
-#pragma unroll
-  for (int n = 1; n < ExpTerms<T>::n; ++n) {
-    const T an = d * c0, bn = a + d * c1, dn = b;
-    a = an;
-    b = bn;
-    d = dn;
-    fact *= T(1) / T(n);
-    // i^n: 1, i, -1, -i
-    const T sgn = ((n >> 1) & 1) ? T(-1) : T(1);
-    if (n & 1) {
-      f0.im += sgn * fact * a;
-      f1.im += sgn * fact * b;
-      f2.im += sgn * fact * d;
-    } else {
-      f0.re += sgn * fact * a;
-      f1.re += sgn * fact * b;
-      f2.re += sgn * fact * d;
-    }
-  }
-  for (int k = 0; k < sq; ++k) {
-    const cx<T> f12 = f1 * f2, f22 = f2 * f2;
-    const cx<T> g0 = f0 * f0 + f12 * (T(2) * c0);
-    const cx<T> g1 = (f0 * f1) * T(2) + f12 * (T(2) * c1) + f22 * c0;
-    const cx<T> g2 = f1 * f1 + (f0 * f2) * T(2) + f22 * c1;
-    f0 = g0;
-    f1 = g1;
-    f2 = g2;
-    c1 *= T(4);
-    c0 *= T(8);
-  }
-  // back to the basis (1, Q, Q^2): Q' = scale Q
-  f1 = f1 * scale;
-  f2 = f2 * (scale * scale);
-  Mat<3, T> R;
-#pragma unroll
-  for (int i = 0; i < 3; ++i)
-#pragma unroll
-    for (int j = 0; j < 3; ++j) {
-      R.e[i][j] = f1 * Q.e[i][j] + f2 * Q2.e[i][j];
-      if (i == j) R.e[i][j] += f0;
-    }
-  return R;
-}
-
-// hermitian traceless Q = s * sum_a h_a lambda_a (Gell-Mann, a = 1..8)
-template <typename T> KLFT_D Mat<3, T> gellmann_combo(const T h[8], T s) {
-  const T r3 = T(1) / sqrt(T(3));
-  Mat<3, T> Q;
-  const T a1 = s * h[0], a2 = s * h[1], a3 = s * h[2], a4 = s * h[3], a5 = s * h[4], a6 = s * h[5], a7 = s * h[6],
-          a8 = s * h[7];
-  Q.e[0][0] = mk<T>(a3 + a8 * r3, T(0));
-  Q.e[1][1] = mk<T>(-a3 + a8 * r3, T(0));
-  Q.e[2][2] = mk<T>(T(-2) * a8 * r3, T(0));
-  Q.e[0][1] = mk<T>(a1, -a2);
-  Q.e[1][0] = mk<T>(a1, a2);
-  Q.e[0][2] = mk<T>(a4, -a5);
-  Q.e[2][0] = mk<T>(a4, a5);
-  Q.e[1][2] = mk<T>(a6, -a7);
-  Q.e[2][1] = mk<T>(a6, a7);
-  return Q;
-}
 
 // ------------------------------------------------------------------ proposals
 // U(1): exp(i phi), phi uniform in [-delta*pi, delta*pi]   (SUN.hpp:163-171)
@@ -152,21 +36,10 @@ template <typename T> KLFT_D Mat<2, T> propose(Stream &g, const Mat<2, T> *, dou
   r.e[1][1] = mk<T>(r.e[0][0].re, -r.e[0][0].im);
   return r;
 }
-// SU(3): reference Gram-Schmidt proposal (SUN.hpp:192-251), or exp(i eps H)
-// with H = sum_a h_a lambda_a / 2, h_a ~ N(0,1) from four Box-Muller pairs.
-template <typename T> KLFT_D Mat<3, T> propose(Stream &g, const Mat<3, T> *, double delta, int proposal, double eps) {
+// SU(3): reference Gram-Schmidt proposal (SUN.hpp:192-251); the exp(i eps H)
+// proposal has its own fixed-position stream (expprop.cuh).
+template <typename T> KLFT_D Mat<3, T> propose(Stream &g, const Mat<3, T> *, double delta, int, double) {
   Mat<3, T> r;
-  if (proposal == PROPOSAL_EXP) {
-    T h[8];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      double a, b;
-      g.gauss2(a, b);
-      h[2 * k] = (T)a;
-      h[2 * k + 1] = (T)b;
-    }
-    return expi_su3(gellmann_combo(h, (T)(0.5 * eps)));
-  }
   T r1[6], r2[6], norm, fact;
   cx<T> z1[3], z2[3], z3[3], z;
   // The rejection loops of the reference end once a draw has nonzero norm; they
@@ -310,7 +183,13 @@ template <typename T> KLFT_D Mat<2, T> expmap(const T *p, T t, const Mat<2, T> *
   return m;
 }
 template <typename T> KLFT_D Mat<3, T> expmap(const T *p, T t, const Mat<3, T> *) {
-  return expi_su3(gellmann_combo(p, t));
+  const XMat<T> x = expi_gellmann<T>(p, t);
+  Mat<3, T> m;
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) m.e[i][j] = mk<T>(x.re[i][j], x.im[i][j]);
+  return m;
 }
 
 }  // namespace klft

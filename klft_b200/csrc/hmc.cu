@@ -248,9 +248,12 @@ klft_status enqueue_energies(klft_lattice *lat, const HmcBufs &b, double *slot_k
 
 // Integrator.hpp:26-53 (reference leapfrog), the standard leapfrog, and the
 // 2nd-order minimum-norm (Omelyan) scheme; then reunitarisation.
+// With t_a / 2 generators a step of length dt moves the links and momenta
+// exactly as a reference step of length dt / 2 (the force halves and the
+// exponent halves), so the HALF normalisation integrates tau / 2.
 klft_status enqueue_integrate(klft_lattice *lat, const HmcBufs &b, double beta, double tau, int nsteps,
                               int integrator) {
-  const double dt = tau / (double)nsteps;
+  const double dt = (lat->hmc_generators == KLFT_GENERATORS_HALF ? 0.5 : 1.0) * tau / (double)nsteps;
   auto P = [&](double h) -> klft_status {
     CK(launch_force_update(lat, b.P, beta, h));
     return KLFT_OK;
@@ -441,7 +444,7 @@ klft_status klft_gauge_force(klft_lattice *lat, double beta, double *host_force)
   klft_status s = hmc_bufs(lat, 1, b);
   if (s != KLFT_OK) return s;
   CK(cudaMemsetAsync(b.P, 0, p_bytes(lat), lat->stream));
-  CK(launch_force_update(lat, b.P, beta, -1.0));
+  CK(launch_force_update(lat, b.P, beta, lat->hmc_generators == KLFT_GENERATORS_HALF ? -0.5 : -1.0));
   const size_t n = (size_t)lat->g.V * lat->g.nd * ncomp_of(lat->nc);
   CK(lat->s_stage.ensure(n * sizeof(double)));
   const unsigned grid = grid_for(lat->g.V * lat->g.nd, 256);
@@ -470,6 +473,15 @@ klft_status klft_hmc_energies(klft_lattice *lat, double beta, double *kinetic, d
   CK(cudaStreamSynchronize(lat->stream));
   if (kinetic) *kinetic = h[0];
   if (gauge_action) *gauge_action = -(beta / (double)lat->nc) * h[1];
+  return KLFT_OK;
+}
+
+klft_status klft_hmc_set_generators(klft_lattice *lat, int generators) {
+  if (!lat) return fail(KLFT_EINVAL, "klft_hmc_set_generators: null handle");
+  if (generators != KLFT_GENERATORS_REFERENCE && generators != KLFT_GENERATORS_HALF)
+    return fail(KLFT_EINVAL, "klft_hmc_set_generators: unknown normalisation %d", generators);
+  std::lock_guard<std::mutex> guard(lat->mtx);
+  lat->hmc_generators = generators;
   return KLFT_OK;
 }
 

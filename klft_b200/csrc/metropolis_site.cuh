@@ -19,65 +19,25 @@
 // Random numbers: the reference proposals (U(1), SU(2), the SU(3)
 // Gram-Schmidt generator) consume the site's sequential Philox stream in the
 // order the reference functor consumes its generator.  The exp(i eps H)
-// proposal (no reference counterpart) reads fixed stream positions per hit (see
-// ExpHitStream), so a proposal does not depend on earlier accept decisions.
-// Neither depends on the launch shape.
+// proposal (no reference counterpart, expprop.cuh) reads fixed stream positions
+// per hit, so a proposal does not depend on earlier accept decisions.  Neither
+// depends on the launch shape.
 #pragma once
+#include <type_traits>
+
+#include "expprop.cuh"
 #include "group.cuh"
 #include "kernels.cuh"
 #include "staple.cuh"
 
+#ifndef KLFT_EXP_PAIRS
+#define KLFT_EXP_PAIRS 1
+#endif
+#ifndef KLFT_EXP_M0_SMEM
+#define KLFT_EXP_M0_SMEM 1
+#endif
+
 namespace klft {
-
-// Fixed-position stream of the exp(i eps H) proposal: hit h of a site
-// (h = mu*nHits + hit) uses Philox blocks 2h, 2h+1 of sub-stream 0 (eight
-// 32-bit uniforms u = (w + 1/2) 2^-32 for four Box-Muller pairs) and word h mod 4
-// of block h / 4 of sub-stream 1 for its accept uniform (w + 1/2) 2^-32, so one
-// block serves the accept decisions of four hits.
-struct ExpHitStream {
-  uint32_t k0, k1, site, step;
-  KLFT_D void block(uint32_t b, uint32_t w[4], uint32_t sub = 0) const {
-    w[0] = b; w[1] = site; w[2] = step; w[3] = (KIND_METROPOLIS << 24) | sub;
-    philox4x32_10(w, k0, k1);
-  }
-  KLFT_D void accept_block(uint32_t h, uint32_t w[4]) const { block(h >> 2, w, 1); }
-};
-
-KLFT_D double accept_word(const uint32_t w[4], uint32_t h) {
-  const uint32_t j = h & 3;
-  const uint32_t x = j == 0 ? w[0] : (j == 1 ? w[1] : (j == 2 ? w[2] : w[3]));
-  return ((double)x + 0.5) * 0x1.0p-32;
-}
-
-KLFT_D void box_muller(uint32_t wa, uint32_t wb, double &g0, double &g1) {
-  const double ua = ((double)wa + 0.5) * 0x1.0p-32, ub = ((double)wb + 0.5) * 0x1.0p-32;
-  const double r = sqrt(-2.0 * log(ua));
-  double s, c;
-  sincospi(2.0 * ub, &s, &c);
-  g0 = r * c;
-  g1 = r * s;
-}
-// Mixed form: SFU log, rsqrt and sincos.  cos/sin(2 pi u) = -cos/sin(2 pi (u - 1/2))
-// keeps the SFU argument in [-pi, pi]; ua rounds to 1 for the largest words,
-// where the radius is 0.
-KLFT_D void box_muller(uint32_t wa, uint32_t wb, float &g0, float &g1) {
-  const float ua = fmaf((float)wa, 0x1.0p-32f, 0x1.0p-33f), ub = fmaf((float)wb, 0x1.0p-32f, 0x1.0p-33f);
-  const float q = -2.0f * __logf(ua);
-  const float r = q > 0.0f ? q * rsqrtf(q) : 0.0f;
-  float s, c;
-  __sincosf(6.28318530717958648f * (ub - 0.5f), &s, &c);
-  g0 = -r * c;
-  g1 = -r * s;
-}
-
-// X = exp(i eps H) of one hit from its eight stream words (blocks 2h, 2h+1)
-template <typename T>
-KLFT_D Mat<3, T> exp_proposal_w(const uint32_t (&w)[8], T half_eps) {
-  T g[8];
-#pragma unroll
-  for (int k = 0; k < 4; ++k) box_muller(w[2 * k], w[2 * k + 1], g[2 * k], g[2 * k + 1]);
-  return expi_su3(gellmann_combo(g, half_eps));
-}
 
 template <int NC, typename T>
 KLFT_D T retr_diag(const Mat<NC, T> &M) {
@@ -191,6 +151,42 @@ KLFT_D int site_update_ref(const Links<NC, T> &U, const Geom &g, const Site &x, 
 // every hit, so this halves the products per hit against carrying U and U S).
 // The link is rebuilt as A U0 and reunitarised once after its hits.  The Markov
 // chain is the one of U <- X U per accepted hit; only the rounding differs.
+//
+// One hit: Y = X A (A is the identity before the first hit), the action
+// change against the current Re Tr(A M0) = trO, the accept test with the hit's
+// FP64 uniform; on acceptance A <- Y.
+// Re Tr(Y M0) with M0 in shared memory (entry (k, i) at mq[(3 k + i) * 128])
+KLFT_D float retr_mul_shared(const Mat<3, float> &Y, const float2 *mq) {
+  float tY = 0.0f;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    const float2 m0 = mq[(0 * 3 + i) * 128], m1 = mq[(1 * 3 + i) * 128], m2 = mq[(2 * 3 + i) * 128];
+    float s = Y.e[i][0].re * m0.x - Y.e[i][0].im * m0.y;
+    s = fmaf(Y.e[i][1].re, m1.x, s);
+    s = fmaf(-Y.e[i][1].im, m1.y, s);
+    s = fmaf(Y.e[i][2].re, m2.x, s);
+    s = fmaf(-Y.e[i][2].im, m2.y, s);
+    tY += s;
+  }
+  return tY;
+}
+
+template <typename T, typename MT>
+KLFT_D void exp_hit(const Mat<3, T> &X, bool first, const MT &M0, T bnc, T cdef, const uint32_t aw[4],
+                    uint32_t h, Mat<3, T> &A, T &trO, int &nacc) {
+  const Mat<3, T> Y = first ? X : mul(X, A);
+  T tY;
+  if constexpr (std::is_same<MT, Mat<3, T>>::value) tY = retr_mul(Y, M0);
+  else tY = retr_mul_shared(Y, M0);
+  const T dS = -bnc * (tY - trO) * cdef;
+  const bool accept = dS < T(0) || accept_word(aw, h) < (double)exp(-dS);
+  if (accept) {
+    A = Y;
+    trO = tY;
+    ++nacc;
+  }
+}
+
 template <int ND, typename T, bool DF>
 KLFT_D int site_update_exp(const Links<3, T> &U, const Geom &g, const Site &x, const MetroArgs &a, uint32_t sweep,
                            const Defect &df) {
@@ -207,39 +203,69 @@ KLFT_D int site_update_exp(const Links<3, T> &U, const Geom &g, const Site &x, c
     // link is A U0 and Re Tr(X A U0 S) = Re Tr((X A) M0): one product X A per hit
     const Mat<3, T> M0 = mul(U.load(lx, mu), staple<3, ND, T, DF>(U, g, x, mu, df));
     Mat<3, T> A = mident<3, T>();
-    const bool dlink = DF && df.active && in_defect(g, df, x, mu);
+    const T cdef = DF && df.active && in_defect(g, df, x, mu) ? (T)defect_c(df) : T(1);
     T trO = retr_diag(M0);
-    bool changed = false;
+    const int nacc0 = nacc;
     uint32_t aw[4];
-    // the Philox words of hit h + 1 are drawn while hit h is evaluated
-    uint32_t wn[8];
-    hs.block(2 * h0, wn);
-    hs.block(2 * h0 + 1, wn + 4);
-#pragma unroll 1
-    for (int hit = 0; hit < a.nhits; ++hit) {
-      const uint32_t h = h0 + (uint32_t)hit;
-      if (hit == 0 || (h & 3u) == 0u) hs.accept_block(h, aw);
-      uint32_t w[8];
+    if constexpr (sizeof(T) == 4 && KLFT_EXP_PAIRS) {
+      // FP32: the proposals of hits h and h + 1 are built together, one hit in
+      // each lane of packed FP32 pairs, then evaluated in turn; the second one
+      // waits in shared memory (one 8-byte complex per entry and thread, so a
+      // warp's accesses are 256 contiguous bytes) while the first is evaluated
+      __shared__ float2 xs[9][128];
+      float2 *xq = &xs[0][threadIdx.x];
+#if KLFT_EXP_M0_SMEM
+      __shared__ float2 ms[9][128];
+      float2 *mq = &ms[0][threadIdx.x];
 #pragma unroll
-      for (int k = 0; k < 8; ++k) w[k] = wn[k];
-      if (hit + 1 < a.nhits) {
-        hs.block(2 * (h + 1), wn);
-        hs.block(2 * (h + 1) + 1, wn + 4);
+      for (int k = 0; k < 9; ++k) mq[k * 128] = make_float2(M0.e[k / 3][k % 3].re, M0.e[k / 3][k % 3].im);
+#endif
+#pragma unroll 1
+      for (int hit = 0; hit < a.nhits; hit += 2) {
+        const uint32_t h = h0 + (uint32_t)hit;
+        const bool two = hit + 1 < a.nhits;
+        Mat<3, T> X;
+        {
+          const XMat<float2> P = exp_proposal_pair(hs, h, half_eps, two);
+#pragma unroll
+          for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+              X.e[i][j] = mk<T>(P.re[i][j].x, P.im[i][j].x);
+              xq[(i * 3 + j) * 128] = make_float2(P.re[i][j].y, P.im[i][j].y);
+            }
+        }
+        if (hit == 0 || (h & 3u) == 0u) hs.accept_block(h, aw);
+#if KLFT_EXP_M0_SMEM
+        exp_hit<T>(X, hit == 0, (const float2 *)mq, bnc, cdef, aw, h, A, trO, nacc);
+#else
+        exp_hit<T>(X, hit == 0, M0, bnc, cdef, aw, h, A, trO, nacc);
+#endif
+        if (two) {
+#pragma unroll
+          for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+              const float2 v = xq[(i * 3 + j) * 128];
+              X.e[i][j] = mk<T>(v.x, v.y);
+            }
+          if (((h + 1u) & 3u) == 0u) hs.accept_block(h + 1u, aw);
+#if KLFT_EXP_M0_SMEM
+          exp_hit<T>(X, false, (const float2 *)mq, bnc, cdef, aw, h + 1u, A, trO, nacc);
+#else
+          exp_hit<T>(X, false, M0, bnc, cdef, aw, h + 1u, A, trO, nacc);
+#endif
+        }
       }
-      const Mat<3, T> X = exp_proposal_w<T>(w, half_eps);
-      const Mat<3, T> Y = hit == 0 ? X : mul(X, A);  // A is the identity before the first hit
-      const T tY = retr_mul(Y, M0);
-      T dS = -bnc * (tY - trO);
-      if (dlink) dS *= (T)defect_c(df);
-      const bool accept = dS < T(0) || accept_word(aw, h) < (double)exp(-dS);
-      if (accept) {
-        A = Y;
-        trO = tY;
-        ++nacc;
-        changed = true;
+    } else {
+#pragma unroll 1
+      for (int hit = 0; hit < a.nhits; ++hit) {
+        const uint32_t h = h0 + (uint32_t)hit;
+        if (hit == 0 || (h & 3u) == 0u) hs.accept_block(h, aw);
+        exp_hit<T>(exp_proposal<T>(hs, h, half_eps), hit == 0, M0, bnc, cdef, aw, h, A, trO, nacc);
       }
     }
-    if (changed) U.store(lx, mu, restore(mul(A, U.load(lx, mu))));
+    if (nacc != nacc0) U.store(lx, mu, restore(mul(A, U.load(lx, mu))));
   }
   return nacc;
 }

@@ -14,7 +14,10 @@
 // array's name as an address: on the first call on a device (with that device
 // current) the entry point asks the runtime for the array's device address with
 // cudaGetSymbolAddress and keeps it for later calls on that device.  That first
-// call should therefore come before any stream capture.
+// call should therefore come before any stream capture.  The first call on a
+// device may also make the CUDA driver load this library's kernels (lazy module
+// loading), which can allocate driver memory once; a warm-up call after the
+// lattice is created leaves every later call allocation-free.
 //
 // All calls on a device share the array and it keeps the last call's contents:
 // each call clears the counters it uses before the sweeps.  Two calls whose GPU
@@ -62,11 +65,8 @@ extern "C" klft_status klft_metropolis_sweeps_noalloc(klft_lattice *lat, double 
                 "klft_metropolis_sweeps_noalloc: nsweeps = %d exceeds the static maximum of %d sweeps per call "
                 "(split the run into several calls)",
                 nsweeps, KLFT_NOALLOC_MAX_SWEEPS);
-  if (proposal != KLFT_PROPOSAL_REFERENCE && proposal != KLFT_PROPOSAL_EXP)
-    return fail(KLFT_EINVAL, "klft_metropolis_sweeps_noalloc: unknown proposal %d", proposal);
-  if (!(delta == delta) || !(eps == eps)) return fail(KLFT_EINVAL, "klft_metropolis_sweeps_noalloc: NaN step size");
-  if (lat->nc == 3 && proposal == KLFT_PROPOSAL_REFERENCE && !(delta > 0.0))
-    return fail(KLFT_EINVAL, "klft_metropolis_sweeps_noalloc: the reference SU(3) proposal needs delta > 0");
+  klft_status v = check_proposal(lat, delta, proposal, eps, "klft_metropolis_sweeps_noalloc");
+  if (v != KLFT_OK) return v;
   if (nsweeps == 0) return KLFT_OK;
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);

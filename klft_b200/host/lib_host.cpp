@@ -153,6 +153,8 @@ bool parseInputFile(const std::string &filename, HMCParams &p) {
     }
     p.precision = parse_choice(h["precision"], "fp64", KLFT_PRECISION_FP64, "mixed", KLFT_PRECISION_MIXED,
                                p.precision);
+    p.generators = parse_choice(h["generators"], "reference", KLFT_GENERATORS_REFERENCE, "half",
+                                KLFT_GENERATORS_HALF, p.generators);
     return true;
   } catch (const std::exception &e) {
     printf("Error parsing input file: %s\n", e.what());
@@ -423,6 +425,11 @@ int HMC(const HMCParams &p) {
     return -1;
   }
   klft_lattice_set_stream(g, (uint64_t)p.seed, 0);
+  if (klft_hmc_set_generators(g, p.generators) != KLFT_OK) {
+    printf("Error: %s\n", klft_last_error());
+    klft_lattice_destroy(g);
+    return -1;
+  }
   double plaq = GaugePlaquette(g);
   std::cout << "Starting Plaquette: " << plaq << std::endl;
   std::cout << "Starting HMC: " << std::endl;

@@ -1,8 +1,9 @@
 // hmc -- the klft `hmc` driver (hmc.cpp:6-80) on libklft_b200.  Same flags
 // (--gauge-group U1|SU2 and now SU3, --ndim, --LX, --LY, --LZ, --LT, --n-traj,
 // --n-steps, --tau, --beta, --seed, --outfilename, --help), plus
-// --integrator reference|leapfrog|omelyan, --precision fp64|mixed and
-// -f <yaml> with an HMCParams block.
+// --integrator reference|leapfrog|omelyan, --precision fp64|mixed,
+// --generators reference|half (klft_hmc_set_generators) and -f <yaml> with an
+// HMCParams block.
 #include <cstdio>
 #include <iostream>
 #include <string>
@@ -31,6 +32,7 @@ int main(int argc, char **argv) {
       std::cout << "--outfilename output filename" << std::endl;
       std::cout << "--integrator reference (default), leapfrog or omelyan" << std::endl;
       std::cout << "--precision fp64 (default) or mixed" << std::endl;
+      std::cout << "--generators reference (default: Pauli / Gell-Mann) or half (t_a/2)" << std::endl;
       std::cout << "-f input file with an HMCParams block" << std::endl;
       return 0;
     }
@@ -54,6 +56,7 @@ int main(int argc, char **argv) {
                      : v == "omelyan" ? KLFT_INTEGRATOR_OMELYAN
                                       : KLFT_INTEGRATOR_REFERENCE_LEAPFROG;
     if (a == "--precision") p.precision = v == "mixed" ? KLFT_PRECISION_MIXED : KLFT_PRECISION_FP64;
+    if (a == "--generators") p.generators = v == "half" ? KLFT_GENERATORS_HALF : KLFT_GENERATORS_REFERENCE;
   }
   return klft::HMC(p) == 0 ? 0 : 1;
 }

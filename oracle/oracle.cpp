@@ -237,11 +237,11 @@ static inline void randsun(Mat<2> &r, Stream &g, double delta, int, double) {
 // Project SU(3) proposal X = exp(i eps H), H = sum_a h_a lambda_a / 2, h_a ~ N(0,1).
 // It has no counterpart in the reference, so its random numbers sit at fixed
 // positions of the (sweep, site) stream: hit h of the site (h = mu*nHits + hit)
-// takes Philox blocks 2h and 2h+1 (sub-stream 0) for eight 32-bit uniforms
-// u = (w + 1/2) 2^-32 (Box-Muller pairs (u0,u1), (u2,u3), (u4,u5), (u6,u7)), and
-// word h mod 4 of block h / 4 of sub-stream 1 for its accept uniform
-// (w + 1/2) 2^-32.  A proposal therefore does not depend on earlier accept
-// decisions.
+// takes Philox block h (sub-stream 0); word k gives the Box-Muller pair of
+// h_{2k+1}, h_{2k+2} from its two 16-bit halves, u = (k + 1/2) 2^-16 (low half
+// for the radius, high half for the angle).  Its accept uniform is word h mod 4
+// of block h / 4 of sub-stream 1, (w + 1/2) 2^-32.  A proposal therefore does
+// not depend on earlier accept decisions.
 struct ExpHit {
   uint32_t key[2], site, step;
   ExpHit(uint64_t seed, uint64_t chain, uint32_t site_, uint32_t step_) : site(site_), step(step_) {
@@ -253,11 +253,11 @@ struct ExpHit {
     philox(ctr, key, out);
   }
   void gauss8(uint32_t h, double g[8]) const {
-    uint32_t w[8];
-    block(2 * h, w);
-    block(2 * h + 1, w + 4);
+    uint32_t w[4];
+    block(h, w);
     for (int k = 0; k < 4; ++k) {
-      const double ua = ((double)w[2 * k] + 0.5) * 0x1.0p-32, ub = ((double)w[2 * k + 1] + 0.5) * 0x1.0p-32;
+      const double ua = ((double)(w[k] & 0xFFFFu) + 0.5) * 0x1.0p-16;
+      const double ub = ((double)(w[k] >> 16) + 0.5) * 0x1.0p-16;
       const double r = std::sqrt(-2.0 * std::log(ua));
       g[2 * k] = r * std::cos(6.283185307179586 * ub);
       g[2 * k + 1] = r * std::sin(6.283185307179586 * ub);
@@ -419,10 +419,23 @@ template <int NC> static Mat<NC> staple(const Field<NC> &F, long s, int mu) {
   return temp;
 }
 
+// Neumaier's compensated sum: the lattice sums of the checker stay accurate to
+// about one rounding of the total at any volume, so that a GPU sum in another
+// order is compared with the exact value rather than with a second rounded one.
+struct CompSum {
+  double s = 0.0, c = 0.0;
+  void add(double x) {
+    const double t = s + x;
+    c += std::fabs(s) >= std::fabs(x) ? (s - t) + x : (x - t) + s;
+    s = t;
+  }
+  double value() const { return s + c; }
+};
+
 // GaugePlaquette.hpp:53-85 per site, :125-132 normalisation (returns real part)
 template <int NC> static double plaquette(const Field<NC> &F, bool normalize) {
   const Geo &g = F.g;
-  cplx total(0.0, 0.0);
+  CompSum total;
   for (long s = 0; s < g.V; ++s) {
     cplx t(0.0, 0.0);
     for (int mu = 0; mu < g.nd; ++mu)
@@ -432,10 +445,11 @@ template <int NC> static double plaquette(const Field<NC> &F, bool normalize) {
         Mat<NC> lnu = mul(F.at(s, nu), F.at(g.shift(s, nu, 1), mu));
         for (int a = 0; a < NC; ++a) for (int b = 0; b < NC; ++b) t += lmu.a[a][b] * std::conj(lnu.a[a][b]);
       }
-    total += t;
+    total.add(t.real());
   }
-  if (normalize) total /= (double)g.V * (double)((g.nd * (g.nd - 1) / 2) * NC);
-  return total.real();
+  double r = total.value();
+  if (normalize) r /= (double)g.V * (double)((g.nd * (g.nd - 1) / 2) * NC);
+  return r;
 }
 
 template <int NC> static Mat<NC> line(const Field<NC> &F, long s, int mu, int len) {
@@ -660,15 +674,22 @@ template <> inline Mat<1> expmapN<1>(const double *p, double t) { return expmap(
 template <> inline Mat<2> expmapN<2>(const double *p, double t) { return expmap2(p, t); }
 template <> inline Mat<3> expmapN<3>(const double *p, double t) { return expmap3(p, t); }
 
+// Generator normalisation of the HMC maps: 1 = the reference's (Pauli /
+// Gell-Mann), 1/2 = t_a / 2.  With t_a / 2 the force is (beta/Nc) Im Tr(t_a U S) / 2
+// and the update exp(i dt sum_a p_a t_a / 2).
+static double g_gen_scale = 1.0;
+
 // GaugeMonomial.hpp:27-37: F(x,mu) = (beta/Nc) Adj(U_mu(x) S_mu(x))
 template <int NC> static void gauge_force(const Field<NC> &F, double beta, double *frc) {
   const int nc = ncomp<NC>();
+  const double fs = (beta / (double)NC) * g_gen_scale;
+#pragma omp parallel for schedule(static) if (F.g.V >= 4096)
   for (long s = 0; s < F.g.V; ++s)
     for (int mu = 0; mu < F.g.nd; ++mu) {
       Mat<NC> M = mul(F.at(s, mu), staple(F, s, mu));
       double v[8];
       adj(M, v);
-      for (int a = 0; a < nc; ++a) frc[(s * F.g.nd + mu) * nc + a] = (beta / (double)NC) * v[a];
+      for (int a = 0; a < nc; ++a) frc[(s * F.g.nd + mu) * nc + a] = fs * v[a];
     }
 }
 
@@ -679,13 +700,14 @@ template <int NC> static double gauge_action(const Field<NC> &F, double beta) {
 
 // HamiltonianField.hpp:40-48
 static double kinetic(const double *P, long n) {
-  double k = 0.0;
-  for (long i = 0; i < n; ++i) k += 0.5 * P[i] * P[i];
-  return k;
+  CompSum k;
+  for (long i = 0; i < n; ++i) k.add(0.5 * P[i] * P[i]);
+  return k.value();
 }
 
 template <int NC> static void momenta(const Geo &g, double *P, uint64_t seed, uint64_t chain, uint32_t traj) {
   const int nc = ncomp<NC>();
+#pragma omp parallel for schedule(static) if (g.V >= 4096)
   for (long s = 0; s < g.V; ++s)
     for (int mu = 0; mu < g.nd; ++mu) {
       Stream st(seed, chain, (uint32_t)s, traj, KIND_MOMENTUM, (uint32_t)mu);
@@ -703,8 +725,10 @@ template <int NC> static void update_momentum(const Field<NC> &F, double *P, dou
 }
 template <int NC> static void update_gauge(const Field<NC> &F, const double *P, double dt) {
   const int nc = ncomp<NC>();
+#pragma omp parallel for schedule(static) if (F.g.V >= 4096)
   for (long s = 0; s < F.g.V; ++s)
-    for (int mu = 0; mu < F.g.nd; ++mu) F.put(s, mu, mul(expmapN<NC>(P + (s * F.g.nd + mu) * nc, dt), F.raw(s, mu)));
+    for (int mu = 0; mu < F.g.nd; ++mu)
+      F.put(s, mu, mul(expmapN<NC>(P + (s * F.g.nd + mu) * nc, dt * g_gen_scale), F.raw(s, mu)));
 }
 
 enum { INTEGRATOR_REFERENCE_LEAPFROG = 0, INTEGRATOR_LEAPFROG = 1, INTEGRATOR_OMELYAN = 2 };
@@ -740,6 +764,7 @@ static void integrate(const Field<NC> &F, double *P, double beta, double tau, in
       update_momentum(F, P, frc.data(), beta, lam * dt);
     }
   }
+#pragma omp parallel for schedule(static) if (F.g.V >= 4096)
   for (long s = 0; s < F.g.V; ++s)
     for (int mu = 0; mu < F.g.nd; ++mu)
       if (!F.g.open_link(s, mu)) F.put(s, mu, restore(F.raw(s, mu)));
@@ -836,6 +861,28 @@ int oracle_uniforms(uint64_t seed, uint64_t chain, uint32_t site, uint32_t step,
 }
 
 void oracle_set_open_boundary(int mu) { g_open_mu = mu; }
+
+// HMC generators for the following calls: 0 = the reference's, 1 = t_a / 2
+void oracle_set_generators(int half) { g_gen_scale = half ? 0.5 : 1.0; }
+
+// The Lie-algebra maps on one matrix (interleaved re/im, row major): Adj(M)
+// and exp(t p) (the reference normalisation), for pinning against klft's code.
+int oracle_adjoint(int nc, const double *M, double *v) {
+  DISPATCH_NC(nc, ({
+    Mat<NC> m;
+    for (int i = 0; i < NC; ++i) for (int j = 0; j < NC; ++j) m.a[i][j] = cplx(M[2 * (i * NC + j)], M[2 * (i * NC + j) + 1]);
+    adj(m, v);
+  }));
+  return 0;
+}
+int oracle_expmap(int nc, const double *p, double t, double *M) {
+  DISPATCH_NC(nc, ({
+    const Mat<NC> m = expmapN<NC>(p, t);
+    for (int i = 0; i < NC; ++i)
+      for (int j = 0; j < NC; ++j) { M[2 * (i * NC + j)] = m.a[i][j].real(); M[2 * (i * NC + j) + 1] = m.a[i][j].imag(); }
+  }));
+  return 0;
+}
 
 int oracle_init(int nc, int nd, const int *L, int hot, uint64_t seed, uint64_t chain, double *U) {
   Geo g(nd, L);

@@ -48,8 +48,9 @@ def build(force: bool = False) -> None:
     if ref_dir:
         if not os.path.isdir(os.path.join(ref_dir, "include")):
             raise FileNotFoundError(f"KLFT_REF_DIR={ref_dir} has no include/ directory")
-        deps = [os.path.join(HERE, "ref_harness.cpp")] + glob.glob(os.path.join(HERE, "ref_shim", "*.hpp"))
-        if force or _stale(REF_SO, deps):
+        deps = [os.path.join(HERE, "ref_harness.cpp"), os.path.join(HERE, "ref_adjoint.cpp")]
+        deps += glob.glob(os.path.join(HERE, "ref_shim", "*.hpp"))
+        if force or _stale(REF_SO, deps) or _stale(os.path.join(HERE, "_ref", "libklft_ref_adjoint.so"), deps):
             subprocess.run(["make", "-C", HERE, "ref", "KLFT_REF_DIR=" + ref_dir], check=True, capture_output=True)
     elif not os.path.exists(REF_SO):
         sys.stderr.write("oracle: KLFT_REF_DIR is not set and oracle/_ref/libklft_ref.so does not exist; "
@@ -111,6 +112,10 @@ class Oracle:
         L.oracle_expi_su3.argtypes = [_dp, _dp]
         L.oracle_set_open_boundary.argtypes = [C.c_int]
         L.oracle_set_open_boundary.restype = None
+        L.oracle_set_generators.argtypes = [C.c_int]
+        L.oracle_set_generators.restype = None
+        L.oracle_adjoint.argtypes = [C.c_int, _dp, _dp]
+        L.oracle_expmap.argtypes = [C.c_int, _dp, C.c_double, _dp]
         L.oracle_gauge_force.argtypes = [C.c_int, C.c_int, _ip, _dp, C.c_double, _dp]
         L.oracle_momenta.argtypes = [C.c_int, C.c_int, _ip, C.c_uint64, C.c_uint64, C.c_uint32, _dp]
         L.oracle_gauge_action.argtypes = [C.c_int, C.c_int, _ip, _dp, C.c_double, _dp]
@@ -200,6 +205,24 @@ class Oracle:
         self.lib.oracle_expi_su3(_d(q), _d(o))
         return o
 
+    def set_generators(self, half: bool) -> None:
+        """HMC generators for the following calls: the reference's, or t_a / 2."""
+        self.lib.oracle_set_generators(int(half))
+
+    def adjoint(self, M):
+        """Adj(M) of one Nc x Nc complex matrix (reference normalisation)."""
+        m = np.ascontiguousarray(M, dtype=np.complex128)
+        v = np.zeros(ncomp(m.shape[0]))
+        self.lib.oracle_adjoint(m.shape[0], _d(m), _d(v))
+        return v
+
+    def expmap(self, nc, p, t):
+        """exp(i t sum_a p_a t_a) in the reference normalisation."""
+        pa = np.ascontiguousarray(p, dtype=np.float64)
+        m = np.zeros((nc, nc), dtype=np.complex128)
+        self.lib.oracle_expmap(nc, _d(pa), t, _d(m))
+        return m
+
     def gauge_force(self, lat: Lat, U, beta):
         f = np.zeros((lat.V, lat.nd, ncomp(lat.nc)))
         self.lib.oracle_gauge_force(lat.nc, lat.nd, _i(lat.Lc), _d(U), beta, _d(f))
@@ -241,6 +264,47 @@ class Oracle:
         o = np.zeros(1)
         self.lib.oracle_unitarity(lat.nc, lat.nd, _i(lat.Lc), _d(U), _d(o))
         return float(o[0])
+
+
+REF_ADJ_SO = os.path.join(HERE, "_ref", "libklft_ref_adjoint.so")
+
+
+class RefAdjoint:
+    """klft's HMC Lie-algebra maps (AdjointGroup.hpp on the SU2 / U1 structs of
+    GaugeGroup.hpp), compiled unchanged on the shim (oracle/_ref)."""
+
+    def __init__(self, path: str = REF_ADJ_SO):
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        self.lib = C.CDLL(path)
+        L = self.lib
+        L.ref_su2_adjoint.argtypes = [_dp, _dp]
+        L.ref_su2_exp.argtypes = [_dp, C.c_double, _dp]
+        L.ref_su2_mul.argtypes = [_dp, _dp, _dp]
+        L.ref_u1_adjoint.argtypes = [_dp, _dp]
+        L.ref_u1_exp.argtypes = [C.c_double, C.c_double, _dp]
+
+    def adjoint(self, M):
+        m = np.ascontiguousarray(M, dtype=np.complex128)
+        v = np.zeros(3 if m.shape[0] == 2 else 1)
+        (self.lib.ref_su2_adjoint if m.shape[0] == 2 else self.lib.ref_u1_adjoint)(_d(m), _d(v))
+        return v
+
+    def expmap(self, nc, p, t):
+        m = np.zeros((nc, nc), dtype=np.complex128)
+        if nc == 2:
+            pa = np.ascontiguousarray(p, dtype=np.float64)
+            self.lib.ref_su2_exp(_d(pa), t, _d(m))
+        else:
+            self.lib.ref_u1_exp(float(np.asarray(p).reshape(-1)[0]), t, _d(m))
+        return m
+
+    def su2_mul(self, A, B):
+        a = np.ascontiguousarray(A, dtype=np.complex128)
+        b = np.ascontiguousarray(B, dtype=np.complex128)
+        c = np.zeros((2, 2), dtype=np.complex128)
+        self.lib.ref_su2_mul(_d(a), _d(b), _d(c))
+        return c
 
 
 class RefShim:

@@ -34,3 +34,12 @@ def has_gpu():
         return klft_b200.device_count() > 0
     except Exception:
         return False
+
+
+@pytest.fixture(scope="session")
+def refadj():
+    from oracle.oracle import REF_ADJ_SO, RefAdjoint, build
+    build()
+    if not os.path.exists(REF_ADJ_SO):
+        pytest.skip("reference adjoint library not built (reference sources were not available at build time)")
+    return RefAdjoint()

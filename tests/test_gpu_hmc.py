@@ -83,3 +83,41 @@ def test_gpu_reversibility_and_mixed_dH():
         out[precision] = g.hmc(2.3, 1.0, 20, 1, "leapfrog")[0][0]
         g.close()
     assert abs(out["fp64"] - out["mixed"]) < 2e-2
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("generators,integrator", [("half", "leapfrog"), ("reference", "omelyan"),
+                                                   ("half", "omelyan")])
+def test_su2_8x4_hmc_chain_accepts_and_exp_minus_dH_is_one(precision, generators, integrator):
+    """SU(2) 8^4 at beta 2.3, tau 1, 20 steps after a Metropolis
+    thermalisation: acceptance above one half and <exp(-dH)> = 1 within three
+    standard errors over 140 trajectories, in both forms.  (klft's Pauli
+    normalisation with the 20-step leapfrog doubles the effective step and
+    accepts about half of the trajectories at this volume, none at 24^4.)"""
+    import klft_b200
+    g = klft_b200.GaugeField([8, 8, 8, 8], 2, precision, "hot", 808)
+    g.set_stream(808, 1)
+    g.metropolis(2.3, 0.3, 5, 100)
+    g.set_hmc_generators(generators)
+    g.hmc(2.3, 1.0, 20, 10, integrator)
+    dH, acc = g.hmc(2.3, 1.0, 20, 140, integrator)
+    e = np.exp(-dH)
+    assert acc.mean() > 0.5
+    assert abs(e.mean() - 1.0) < 3.0 * e.std(ddof=1) / np.sqrt(len(e))
+    assert 0.55 < g.plaquette() < 0.65
+    g.close()
+
+
+def test_half_generators_are_the_reference_at_half_tau_on_gpu():
+    import klft_b200
+    out = []
+    for generators, tau in (("half", 0.8), ("reference", 0.4)):
+        g = klft_b200.GaugeField([4, 4, 4, 6], 3, "fp64", "hot", 77)
+        g.set_hmc_generators(generators)
+        g.set_stream(3, 0)
+        dH, acc = g.hmc(5.5, tau, 6, 3, "omelyan")
+        out.append((dH, acc, g.download()))
+        g.close()
+    np.testing.assert_array_equal(out[0][0], out[1][0])
+    np.testing.assert_array_equal(out[0][1], out[1][1])
+    np.testing.assert_array_equal(out[0][2], out[1][2])

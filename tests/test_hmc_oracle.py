@@ -72,3 +72,45 @@ def test_force_is_minus_action_gradient(oracle, nc):
             vals.append(oracle.gauge_action(lat, V, beta))
         grad = (vals[0] - vals[1]) / (2 * h)
         assert grad == pytest.approx(F[s, mu, a], rel=1e-5, abs=1e-8)
+
+
+@pytest.mark.parametrize("nc", [1, 2, 3])
+@pytest.mark.parametrize("integ", [INTEGRATOR_REFERENCE_LEAPFROG, INTEGRATOR_LEAPFROG, INTEGRATOR_OMELYAN])
+def test_half_generators_equal_reference_at_half_tau(oracle, nc, integ):
+    """t_a / 2 generators (force halved, exponent halved) integrate exactly the
+    reference trajectory of half the length: the scale 1/2 is exact in binary,
+    so the two agree bit for bit."""
+    lat = Lat(nc, [4, 4, 2, 4])
+    U0 = oracle.init(lat, True, 17)
+    P0 = oracle.momenta(lat, 18, 0, 0)
+    Ua, Pa, Ub, Pb = U0.copy(), P0.copy(), U0.copy(), P0.copy()
+    try:
+        oracle.set_generators(True)
+        oracle.integrate(lat, Ua, Pa, 2.1, 0.8, 4, integ)
+        Fh = oracle.gauge_force(lat, U0, 2.1)
+    finally:
+        oracle.set_generators(False)
+    oracle.integrate(lat, Ub, Pb, 2.1, 0.4, 4, integ)
+    assert np.array_equal(Ua, Ub) and np.array_equal(Pa, Pb)
+    assert np.array_equal(Fh, 0.5 * oracle.gauge_force(lat, U0, 2.1))
+
+
+def test_half_generators_accept_more_at_the_same_step_count(oracle):
+    """SU(2) at beta 2.3, tau 1, 10 leapfrog steps: the t_a / 2 normalisation
+    (half the effective step) gives a smaller |dH| than klft's Pauli one, and
+    <exp(-dH)> stays 1 within errors."""
+    lat = Lat(2, [4, 4, 4, 4])
+    out = {}
+    for half in (False, True):
+        U = oracle.init(lat, True, 23)
+        oracle.metropolis(lat, U, 2.3, 0.3, 5, 20, 23)
+        try:
+            oracle.set_generators(half)
+            dH, acc = oracle.hmc(lat, U, 2.3, 1.0, 10, INTEGRATOR_LEAPFROG, 24, 0, 0, 60)
+        finally:
+            oracle.set_generators(False)
+        out[half] = (np.mean(np.abs(dH)), acc.mean(), np.exp(-dH))
+    assert out[True][0] < 0.25 * out[False][0]
+    assert out[True][1] >= out[False][1]
+    e = out[True][2]
+    assert abs(e.mean() - 1.0) < 4 * e.std() / np.sqrt(len(e)) + 1e-3
