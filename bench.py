@@ -211,16 +211,53 @@ def e2e_public_api(g, eps, steps):
     return dt, h2d, d2h
 
 
-def e2e_host_lattice(g, eps, steps):
-    """Per step: upload links from host, cycle, download links (users keeping configs on the host)."""
-    U = g.download()
+def host_buffer(shape, pinned):
+    """A complex128 host array: page-locked (through torch) or ordinary numpy."""
+    if pinned:
+        import torch
+        n = int(np.prod(shape))
+        return torch.empty(n, dtype=torch.complex128, pin_memory=True).numpy().reshape(shape)
+    a = np.empty(shape, dtype=np.complex128)
+    a.fill(0)  # touch the pages before timing
+    return a
+
+
+def e2e_host_lattice(g, eps, steps, pinned=False):
+    """Per step: upload links from host, cycle, download links (users keeping
+    configurations on the host), with one reused host buffer."""
+    U = host_buffer(g.shape(), pinned)
+    g.download(U)
+    g.upload(U)  # warm-up: staging buffers and pages
     t0 = time.perf_counter()
     for _ in range(steps):
         g.upload(U)
         g.run_cycles(BETA, 0.0, NHITS, 1, "exp", eps, True, PAIRS)
-        U = g.download()
+        g.download(U)
     dt = time.perf_counter() - t0
     return dt, U.nbytes, U.nbytes
+
+
+def host_io_rates(g, reps=3):
+    """klft_lattice_upload / klft_lattice_download rates (GB/s of the FP64
+    interchange array), from ordinary and from page-locked host memory."""
+    out = {"bytes": int(np.prod(g.shape())) * 16}
+    for pinned in (False, True):
+        U = host_buffer(g.shape(), pinned)
+        g.download(U)
+        g.upload(U)
+        up, down = [], []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            g.upload(U)
+            t1 = time.perf_counter()
+            g.download(U)
+            t2 = time.perf_counter()
+            up.append(t1 - t0)
+            down.append(t2 - t1)
+        key = "pinned" if pinned else "pageable"
+        out[f"upload_gbs_{key}"] = out["bytes"] / min(up) / 1e9
+        out[f"download_gbs_{key}"] = out["bytes"] / min(down) / 1e9
+    return out
 
 
 def peak(dtype):
@@ -257,23 +294,25 @@ def cpu_baseline_reference(L: int):
                       f"{dt:.2f} s"}
 
 
-# DRAM traffic of one parity pass (dram__bytes_read.sum + dram__bytes_write.sum of one
+# DRAM traffic of one link pass (dram__bytes_read.sum + dram__bytes_write.sum of one
 # metropolis_exp_kernel launch in the ncu capture summarised in the profile below).
-TRAFFIC_PASS_BYTES = 112657920
+TRAFFIC_PASS_BYTES = None
 TRAFFIC_SOURCE = "profiles/metropolis_exp_su3_32x4_mixed.md"
 
 
 def sweep_flops_per_link_update(nhits: int, acceptance: float) -> float:
     """Algorithmic flops of one SU(3) exp(i eps H) link update (6 per complex
-    multiply, 2 per complex add, 198 per 3x3 product): staple 2466, M0 = U0 S 198,
-    per hit the proposal (8 Box-Muller normals 32, Gell-Mann sum 16, Q^2 132,
-    c0/c1 30, 12-term coefficient series 108, X = f0 + f1 Q + f2 Q^2 126), the
-    product X A with the accepted proposals 198 and Re Tr(X A M0) 36; then the
-    link A U0 198 and one reunitarisation (~100).  The accept rate no longer
-    enters: the one product per hit is also the accepted A."""
+    multiply, 2 per complex add, 198 per 3x3 product; an FMA counts 2): staple
+    2466, M0 = U0 S 198, per hit the proposal (8 Box-Muller normals 32, the
+    Gell-Mann coefficients 8, c1 and c0 = det Q 47, the 12-term coefficient
+    series 99, Q^2 from the coefficients 35, X = f0 + f1 Q + f2 Q^2 with its
+    hermitian pairs 75) and Re Tr(X A M0) 36, the product X A on every hit but
+    the first (A is the identity there) 198; then the link A U0 198 and one
+    reunitarisation (~100).  The accept rate does not enter: the one product
+    per hit is also the accepted A."""
     del acceptance
-    proposal = 32 + 16 + 132 + 30 + 108 + 126
-    return 2466 + 198 + nhits * (proposal + 198 + 36) + 198 + 100
+    proposal = 32 + 8 + 47 + 99 + 35 + 75
+    return 2466 + 198 + nhits * (proposal + 36) + (nhits - 1) * 198 + 198 + 100
 
 
 def mixed_errors(g, L):
@@ -408,6 +447,69 @@ def bench_hmc(ntraj: int, cpu: bool = True):
     return out
 
 
+C1_TEMPORAL = [(2, 2), (3, 4), (4, 3), (4, 4)]
+C1_PLANES = [(0, 1), (1, 2), (3, 2)]
+C1_PLANAR = [(2, 2), (3, 3), (4, 3)]
+
+
+def bench_c1(cpu: bool = True):
+    """The small plain-method workload: U(1) 4D 8^4, hot start (phases uniform in
+    [-pi, pi) from seed 32091), Metropolis beta 2, delta 0.1, nHits 10, 1000
+    sweeps, plaquette and the listed temporal and planar Wilson loops every 10
+    sweeps (step 0 excluded).  The GPU runs the FP64 form through the public
+    API (wall clock, host results every measurement); klft's own code runs the
+    same chain on the host cores, on one thread and on all of them.  Both
+    follow the same random stream, so their final plaquettes agree to
+    rounding."""
+    import klft_b200
+    L = [8, 8, 8, 8]
+    V = 8 ** 4
+    g = klft_b200.GaugeField(L, 1, "fp64", "hot", 32091)
+    U0 = g.download()
+    g.set_stream(32091, 0)
+
+    def run_gpu():
+        for _ in range(100):
+            g.metropolis(2.0, 0.1, 10, 10)
+            g.plaquette()
+            g.wilson_loop_temporal(C1_TEMPORAL)
+            for m, n in C1_PLANES:
+                g.wilson_loop_mu_nu(m, n, C1_PLANAR)
+
+    run_gpu()  # warm-up on a copy of the chain
+    g.upload(U0)
+    g.set_counters(0, 0)
+    t0 = time.perf_counter()
+    run_gpu()
+    dt = time.perf_counter() - t0
+    out = {"workload": "U(1) 4D 8^4, hot start seed 32091, beta 2, delta 0.1, nHits 10, 1000 sweeps, plaquette + "
+                       "W_temp (2,2),(3,4),(4,3),(4,4) + W_mu_nu (0,1),(1,2),(3,2) x (2,2),(3,3),(4,3) every 10",
+           "gpu": {"seconds": dt, "link_updates_per_s": 1000 * V * 4 / dt, "plaquette": g.plaquette(),
+                   "path": "GaugeField.metropolis / plaquette / wilson_loop_* (C ABI), FP64, wall clock"}}
+    g.close()
+    if cpu:
+        from oracle.oracle import REF_SO, Lat, RefShim
+        if os.path.exists(REF_SO):
+            r = RefShim()
+            lat = Lat(1, L)
+            for nt in (1, os.cpu_count() or 1):
+                cores = r.set_threads(nt)
+                U = U0.copy()
+                t0 = time.perf_counter()
+                for k in range(100):
+                    r.metropolis(lat, U, 2.0, 0.1, 10, 10, 32091, sweep0=10 * k)
+                    r.plaquette(lat, U)
+                    r.wilson_temporal(lat, U, C1_TEMPORAL)
+                    for m, n in C1_PLANES:
+                        r.wilson_mu_nu(lat, U, m, n, C1_PLANAR)
+                dt = time.perf_counter() - t0
+                out[f"cpu_reference_{cores}_threads"] = {
+                    "seconds": dt, "link_updates_per_s": 1000 * V * 4 / dt, "plaquette": r.plaquette(lat, U),
+                    "kind": "reference", "cores": cores,
+                    "sample": "the whole workload, klft's headers on the project's Kokkos-API OpenMP shim"}
+    return out
+
+
 def bench_serving(njobs: int, rate: float):
     """A seeded Poisson stream of mixed jobs through the job server."""
     from klft_b200.serve import Server, latency_summary, poisson_jobs, run_stream
@@ -452,10 +554,12 @@ def run_ours(a, dist: Dist):
     hbm = pk.get("hbm_gbs")
     fp32 = peak(1)
     fp64 = peak(0)
-    # read + write one FP32 SU(3) link, stored as two rows (12 reals)
+    # read + write one FP32 SU(3) link, stored as two rows (12 reals); a sweep
+    # of the exp proposal is 8 link passes of V/2 links each
     bytes_link_mixed = 2 * 6 * 8
-    pass_ms = ms_sweep / 16.0
-    units_per_launch = V // 16 * 4
+    npass = 2 * 4
+    pass_ms = ms_sweep / npass
+    units_per_launch = V // 2
     achieved = units_per_launch * bytes_link_mixed / (pass_ms * 1e-3) / 1e9
     flop_lu = sweep_flops_per_link_update(NHITS, float(np.mean(acc)))
     tflops = units_per_launch * flop_lu / (pass_ms * 1e-3) / 1e12
@@ -479,11 +583,16 @@ def run_ours(a, dist: Dist):
            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
            "path": "klft_metropolis_sweeps + klft_plaquette + klft_wilson_loop_temporal per step, host wall clock"}
     dist.barrier()
-    hl_dt, hb, db = e2e_host_lattice(g, eps, 2)
+    hl_dt, hb, db = e2e_host_lattice(g, eps, 3)
     hl_dt = dist.max(hl_dt)
-    e2e_host = {"value": links_per_step * 2 * dist.world / hl_dt, "unit": "link updates/s",
+    dist.barrier()
+    hp_dt, _, _ = e2e_host_lattice(g, eps, 3, pinned=True)
+    hp_dt = dist.max(hp_dt)
+    e2e_host = {"value": links_per_step * 3 * dist.world / hl_dt, "unit": "link updates/s",
                 "h2d_bytes_per_step": hb, "d2h_bytes_per_step": db,
-                "path": "upload links + cycle + download links per step"}
+                "path": "upload links + cycle + download links per step, one reused ordinary (pageable) host array",
+                "value_pinned_host": links_per_step * 3 * dist.world / hp_dt,
+                "host_io": host_io_rates(g)}
     # FP64 form from the same thermalised configuration
     fp64_line = None
     if not a.no_fp64:
@@ -498,9 +607,9 @@ def run_ours(a, dist: Dist):
                      "ms_sweep": s64, "ms_measure": m64, "mean_plaquette": float(np.mean(plaq64))}
         g64.close()
     mixed_err = mixed_errors(g, L)
-    # 16 parity passes + counter advance + plaquette and its reduction + the axial-gauge
+    # 8 link passes + counter advance + plaquette and its reduction + the axial-gauge
     # transform (once, shared by the spatial planes) + 3 planes x (U', loops, reduction)
-    launches_per_step = 16 + 1 + 2 + 1 + 3 * 3
+    launches_per_step = npass + 1 + 2 + 1 + 3 * 3
     line = {
         "metric": METRIC, "value": value, "unit": "link updates/s", "n_gpus": dist.world, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak",
@@ -520,7 +629,8 @@ def run_ours(a, dist: Dist):
     line["plaquettes_per_s"] = {"value": V * 6 / (pl_ms * 1e-3), "ms": pl_ms,
                                 "note": "V*Nd(Nd-1)/2 plaquettes per GaugePlaquette, device time"}
     if dist.world == 1 and not a.no_extras:
-        for key, fn in (("batched_ptbc", lambda: bench_batched_ptbc(a.batch_cycles)),
+        for key, fn in (("c1_u1_8x4", lambda: bench_c1(not a.no_cpu_baseline)),
+                        ("batched_ptbc", lambda: bench_batched_ptbc(a.batch_cycles)),
                         ("hmc", lambda: bench_hmc(a.hmc_traj, not a.no_cpu_baseline)),
                         ("serving", lambda: bench_serving(a.serve_jobs, a.serve_rate))):
             try:

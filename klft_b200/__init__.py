@@ -18,7 +18,7 @@ from __future__ import annotations
 import ctypes as C
 import os
 from dataclasses import dataclass, field
-from typing import List, Sequence, Tuple
+from typing import Optional, List, Sequence, Tuple
 
 import numpy as np
 
@@ -118,10 +118,14 @@ class GaugeField:
         assert a.size == self.V * self.nd * self.nc * self.nc
         check(lib().klft_lattice_upload(self._h, a.ctypes.data_as(C.POINTER(C.c_double))))
 
-    def download(self) -> np.ndarray:
-        a = np.zeros(self.shape(), dtype=np.complex128)
-        check(lib().klft_lattice_download(self._h, a.ctypes.data_as(C.POINTER(C.c_double))))
-        return a
+    def download(self, out: Optional[np.ndarray] = None) -> np.ndarray:
+        """The links in the host interchange layout; into `out` (a C-contiguous
+        complex128 array of shape()) when given, e.g. a reused or page-locked buffer."""
+        if out is None:
+            out = np.empty(self.shape(), dtype=np.complex128)
+        assert out.dtype == np.complex128 and out.flags.c_contiguous and out.size == int(np.prod(self.shape()))
+        check(lib().klft_lattice_download(self._h, out.ctypes.data_as(C.POINTER(C.c_double))))
+        return out
 
     def set_stream(self, seed: int, chain: int = 0) -> None:
         check(lib().klft_lattice_set_stream(self._h, seed, chain))
@@ -258,6 +262,14 @@ class GaugeField:
         o = C.c_double()
         check(lib().klft_unitarity(self._h, C.byref(o)))
         return o.value
+
+    def exp_dS_error(self, beta: float, eps: float, nhits: int) -> dict:
+        """FP32 (mixed form) against FP64 action changes of the current sweep's
+        exp(i eps H) proposals on this FP64 SU(3) configuration."""
+        o = np.zeros(6)
+        check(lib().klft_exp_proposal_dS_error(self._h, beta, eps, nhits, o.ctypes.data_as(C.POINTER(C.c_double))))
+        return {"hits": int(o[0]), "mean": o[1], "rms": o[2], "max_abs": o[3], "slope": o[4],
+                "decision_flip_fraction": o[5]}
 
     def reunitarize(self) -> None:
         check(lib().klft_reunitarize(self._h))

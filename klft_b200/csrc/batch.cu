@@ -7,9 +7,11 @@
 // A group's chain table travels by value in the kernel parameters (up to
 // BATCH_MAX chains, read from the constant bank); its CTAs are laid out chain
 // after chain, and a CTA finds its chain by a binary search on the table's
-// block offsets.  Parity classes are the unit of ordering: for each class val
-// one launch per group updates that class of every chain in the group, so the
-// reference's sweep order holds for every chain.  Per-cycle results (accepted
+// block offsets.  Passes are the unit of ordering: for each pass val (a parity
+// class of sites for the reference proposals, a link pass (mu, parity) for the
+// SU(3) exp(i eps H) proposal) one launch per group updates that pass of every
+// chain in the group, so every chain is swept in the order it is swept alone.
+// Per-cycle results (accepted
 // hits, plaquette sums, replica labels) land in device slots selected by a
 // device counter, so the captured graph is replayed unchanged.  Replica swaps
 // run on the device (ptbc.cu) and write each replica's defect coefficient,
@@ -66,11 +68,12 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::v)
   const ChainDesc &c = tab.c[ci];
   const long long t = (long long)(blockIdx.x - c.block_begin) * blockDim.x + threadIdx.x;
   int nacc = 0;
-  if (t < c.g.Vh) {
-    const Links<NC, T> U{(cx<T> *)c.links, c.g.V};
-    const Site x = pass_site(c.g, t, val, ND);
-    if constexpr (EXP && NC == 3) nacc = site_update_exp<ND, T, DF>(U, c.g, x, c.a, *c.ctr, c.df);
-    else nacc = site_update_ref<NC, ND, T, DF>(U, c.g, x, c.a, *c.ctr, c.df);
+  const Links<NC, T> U{(cx<T> *)c.links, c.g.V};
+  if constexpr (EXP && NC == 3) {
+    if (t < c.g.V / 2)
+      nacc = link_update_exp<ND, T, DF>(U, c.g, link_pass_site(c.g, t, val & 1, ND), val >> 1, c.a, *c.ctr, c.df);
+  } else {
+    if (t < c.g.Vh) nacc = site_update_ref<NC, ND, T, DF>(U, c.g, pass_site(c.g, t, val, ND), c.a, *c.ctr, c.df);
   }
   add_accepts(nacc, nacc_slots + (size_t)(*slot) * tab.nchains_total + c.index);
 }
@@ -337,7 +340,7 @@ struct Group {
 
 namespace klft {
 
-// One sweep of every item, interleaved by parity class, in multi-chain launches
+// One sweep of every item, interleaved by pass, in multi-chain launches
 // on stream st.  Accepted hits of item i go to nacc[(*slot) * stride + index],
 // index = items[i].acc_index (i when negative), stride = acc_stride (n when 0);
 // the caller advances the items' sweep counters afterwards.
@@ -375,10 +378,15 @@ klft_status enqueue_multi_sweep(const std::vector<SweepItem> &items, unsigned lo
     d.df = it.df;
     d.index = it.acc_index >= 0 ? it.acc_index : i;
     d.block_begin = grp->blocks.back();
-    grp->blocks.back() += (int)((lat->g.Vh + block - 1) / block);
+    // exp groups: V/2 links per link pass; reference groups: Vh sites per class
+    const long long nthr = key.exp ? lat->g.V / 2 : lat->g.Vh;
+    grp->blocks.back() += (int)((nthr + block - 1) / block);
   }
-  int maxnd = 0;
-  for (auto &gg : groups) maxnd = gg.key.nd > maxnd ? gg.key.nd : maxnd;
+  int maxpass = 0;
+  for (auto &gg : groups) {
+    const int np = gg.key.exp ? 2 * gg.key.nd : 1 << gg.key.nd;
+    maxpass = np > maxpass ? np : maxpass;
+  }
   const int ng = (int)groups.size();
   const int nside = fork && ng > 1 ? std::min(fork->nside, ng - 1) : 0;
   if (nside > 0) {
@@ -387,10 +395,10 @@ klft_status enqueue_multi_sweep(const std::vector<SweepItem> &items, unsigned lo
   }
   // the side streams are joined back even when a launch fails
   cudaError_t err = cudaSuccess;
-  for (int val = 0; val < (1 << maxnd) && err == cudaSuccess; ++val)
+  for (int val = 0; val < maxpass && err == cudaSuccess; ++val)
     for (int gi = 0; gi < ng && err == cudaSuccess; ++gi) {
       const Group &gg = groups[gi];
-      if (val >= (1 << gg.key.nd)) continue;
+      if (val >= (gg.key.exp ? 2 * gg.key.nd : 1 << gg.key.nd)) continue;
       const cudaStream_t gs = gi == 0 || nside == 0 ? st : fork->side[(gi - 1) % nside];
       for (size_t t = 0; t < gg.tables.size() && err == cudaSuccess; ++t) {
         err = launch_group(gg.key, *gg.tables[t], gg.blocks[t], val, nacc, slot, gs);

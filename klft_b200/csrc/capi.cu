@@ -292,7 +292,7 @@ klft_status klft_lattice_upload(klft_lattice *lat, const double *host) {
   LOCK(lat);
   const size_t bytes = (size_t)lat->g.V * lat->g.nd * lat->nc * lat->nc * 16;
   CK(lat->s_stage.ensure(bytes));
-  CK(cudaMemcpyAsync(lat->s_stage.ptr, host, bytes, cudaMemcpyHostToDevice, lat->stream));
+  CK(copy_host_to_device(lat->s_stage.ptr, host, bytes, lat->stream));
   CK(launch_import(lat->nc, lat->dtype(), lat->links, lat->g, (const double *)lat->s_stage.ptr, lat->stream));
   CK(launch_open_boundary(lat->nc, lat->dtype(), lat->links, lat->g, lat->stream));
   CK(cudaStreamSynchronize(lat->stream));
@@ -321,8 +321,7 @@ klft_status klft_lattice_download(klft_lattice *lat, double *host) {
   const size_t bytes = (size_t)lat->g.V * lat->g.nd * lat->nc * lat->nc * 16;
   CK(lat->s_stage.ensure(bytes));
   CK(launch_export(lat->nc, lat->dtype(), lat->links, lat->g, (double *)lat->s_stage.ptr, lat->stream));
-  CK(cudaMemcpyAsync(host, lat->s_stage.ptr, bytes, cudaMemcpyDeviceToHost, lat->stream));
-  CK(cudaStreamSynchronize(lat->stream));
+  CK(copy_device_to_host(host, lat->s_stage.ptr, bytes, lat->stream));
   return KLFT_OK;
 }
 
@@ -573,10 +572,10 @@ static int sweep_block(klft_lattice *lat, const MetroArgs &a, const Defect &df, 
 klft_status enqueue_sweeps(klft_lattice *lat, double beta, double delta, int nhits, int proposal, double eps,
                            int nsweeps, unsigned long long *d_nacc, const Defect &df, bool may_tune) {
   MetroArgs a{beta, delta, eps, nhits, proposal, lat->seed, lat->chain};
-  const int nclass = 1 << lat->g.nd;
+  const int npass = metropolis_passes(lat->nc, proposal, lat->g.nd);
   const int block = sweep_block(lat, a, df, may_tune);
   for (int k = 0; k < nsweeps; ++k) {
-    for (int val = 0; val < nclass; ++val)
+    for (int val = 0; val < npass; ++val)
       CK(launch_metropolis_pass(lat->nc, lat->dtype(), lat->links, lat->g, val, a, lat->d_counters, d_nacc + k, df,
                                 block, lat->stream));
     CK(launch_advance(lat->d_counters, lat->stream));

@@ -31,6 +31,13 @@ double *pinned_slots_get();
 void pinned_slots_put(double *p);
 // The device's default memory pool keeps freed memory for reuse (once per device).
 void keep_pool_memory(int device);
+// Whole-lattice host <-> device copies (hostio.cu): one DMA transfer for a
+// page-locked host buffer, else chunks through the library's page-locked
+// staging buffers filled and drained by host threads.  Both return after the
+// host buffer may be reused (host -> device: the device copy is enqueued on st
+// and complete; device -> host: the data is in dst).
+cudaError_t copy_host_to_device(void *dst, const void *src, size_t bytes, cudaStream_t st);
+cudaError_t copy_device_to_host(void *dst, const void *src, size_t bytes, cudaStream_t st);
 
 klft_status fail(klft_status code, const char *fmt, ...);
 klft_status cuda_fail(cudaError_t e, const char *what);

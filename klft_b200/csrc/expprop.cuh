@@ -15,16 +15,14 @@
 // The exponential is evaluated in the Cayley-Hamilton basis (1, Q, Q^2),
 // Q = (eps/2) sum_a h_a lambda_a, with the Gell-Mann structure written out:
 // Q^2, Tr Q^2 / 2 and det Q come straight from the eight coefficients.  The
-// arithmetic is written once for a "lane" type V: double or float (one
-// proposal), or float2, where the two halves of every packed FP32 register
-// pair carry the proposals of two consecutive hits and each operation is one
-// sm_100 packed instruction (fma.rn.f32x2 and friends).
+// arithmetic is written once for the value type V (double: FP64 form, float:
+// mixed form) through the small v* helpers.
 #pragma once
 #include "common.cuh"
 
 namespace klft {
 
-// ------------------------------------------------------------------ lane arithmetic
+// ------------------------------------------------------------------ arithmetic helpers
 KLFT_D double vfma(double a, double b, double c) { return fma(a, b, c); }
 KLFT_D double vmul(double a, double b) { return a * b; }
 KLFT_D double vadd(double a, double b) { return a + b; }
@@ -33,23 +31,11 @@ KLFT_D float vfma(float a, float b, float c) { return fmaf(a, b, c); }
 KLFT_D float vmul(float a, float b) { return a * b; }
 KLFT_D float vadd(float a, float b) { return a + b; }
 KLFT_D float vsub(float a, float b) { return a - b; }
-KLFT_D float2 vfma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
-KLFT_D float2 vmul(float2 a, float2 b) { return __fmul2_rn(a, b); }
-KLFT_D float2 vadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
-KLFT_D float2 vsub(float2 a, float2 b) {
-  unsigned long long r;
-  asm("sub.rn.f32x2 %0, %1, %2;"
-      : "=l"(r)
-      : "l"(*reinterpret_cast<const unsigned long long *>(&a)), "l"(*reinterpret_cast<const unsigned long long *>(&b)));
-  return *reinterpret_cast<float2 *>(&r);
-}
 template <typename V> KLFT_D V splat(double c);
 template <> KLFT_D double splat<double>(double c) { return c; }
 template <> KLFT_D float splat<float>(double c) { return (float)c; }
-template <> KLFT_D float2 splat<float2>(double c) { return make_float2((float)c, (float)c); }
 KLFT_D double vmax(double a) { return a; }
 KLFT_D float vmax(float a) { return a; }
-KLFT_D float vmax(float2 a) { return fmaxf(a.x, a.y); }
 
 // Terms of the coefficient series: |lambda| <= 1 after scaling, so 1/12! < 3e-9
 // in FP32 and 1/19! < 1e-17 in FP64.
@@ -64,7 +50,7 @@ template <typename V> struct XMat { V re[3][3], im[3][3]; };
 // (d c0, a + d c1, b), and exp(iQ) = f0 + f1 Q + f2 Q^2 with
 // f = sum_n i^n / n! (a_n, b_n, d_n).  Arguments with c1 > 3/4 (an eigenvalue
 // possibly above 1: |lambda|^2 <= 4 c1 / 3) are scaled by 2^-k and the result
-// squared k times in coefficient space (both lanes of a pair by the larger k):
+// squared k times in coefficient space:
 //   (f0 + f1 Q + f2 Q^2)^2 = (f0^2 + 2 f1 f2 c0) + (2 f0 f1 + 2 f1 f2 c1 + f2^2 c0) Q
 //                          + (f1^2 + 2 f0 f2 + f2^2 c1) Q^2.
 template <typename V> KLFT_D XMat<V> expi_gellmann(const V h[8], V s) {
@@ -245,22 +231,6 @@ template <typename T> KLFT_D Mat<3, T> exp_proposal(const ExpHitStream &hs, uint
 #pragma unroll
     for (int j = 0; j < 3; ++j) X.e[i][j] = mk<T>(x.re[i][j], x.im[i][j]);
   return X;
-}
-
-// X of hits h and h + 1 in the two lanes of packed FP32 pairs (FP32 only)
-KLFT_D XMat<float2> exp_proposal_pair(const ExpHitStream &hs, uint32_t h, float half_eps, bool second) {
-  float g0[8], g1[8];
-  hs.gauss8<float>(h, g0);
-  if (second) {
-    hs.gauss8<float>(h + 1, g1);
-  } else {
-#pragma unroll
-    for (int k = 0; k < 8; ++k) g1[k] = 0.0f;
-  }
-  float2 g[8];
-#pragma unroll
-  for (int k = 0; k < 8; ++k) g[k] = make_float2(g0[k], g1[k]);
-  return expi_gellmann<float2>(g, make_float2(half_eps, half_eps));
 }
 
 }  // namespace klft

@@ -1,0 +1,202 @@
+// hostio.cu -- host <-> device copies of whole lattices (klft_lattice_upload /
+// klft_lattice_download; GaugeField.hpp:30-141 keeps its fields in host-visible
+// Kokkos views, so callers of the reference hand configurations around as host
+// arrays).
+//
+// A host buffer that is page-locked (cudaHostAlloc / cudaHostRegister) is copied
+// by one DMA transfer.  An ordinary pageable buffer would otherwise go through
+// the driver's own single-threaded staging, at a fraction of the PCIe rate, so
+// it is copied here in chunks through two page-locked staging buffers owned by
+// the library: host threads fill (or drain) one buffer while the DMA engine
+// moves the other, and the device-side layout conversion runs on the device
+// copy afterwards.  The staging buffers (2 x 32 MB) are allocated on first use
+// and kept for the life of the process.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <condition_variable>
+#include <cstring>
+#include <functional>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "capi_internal.h"
+
+namespace klft {
+namespace {
+
+constexpr size_t kChunk = 32u << 20;
+
+// A small persistent pool of host threads for the staging memcpys.
+class CopyPool {
+ public:
+  static CopyPool &get() {
+    static CopyPool p;
+    return p;
+  }
+  // fn(i) for i in [0, n) on the pool threads and the caller
+  void run(int n, const std::function<void(int)> &fn) {
+    if (n <= 1 || workers_.empty()) {
+      for (int i = 0; i < n; ++i) fn(i);
+      return;
+    }
+    std::unique_lock<std::mutex> lk(mu_);
+    fn_ = &fn;
+    next_ = 0;
+    n_ = n;
+    done_ = 0;
+    ++gen_;
+    cv_.notify_all();
+    lk.unlock();
+    work();
+    lk.lock();
+    done_cv_.wait(lk, [&] { return done_ == n_; });
+    fn_ = nullptr;
+  }
+  int threads() const { return (int)workers_.size() + 1; }
+
+ private:
+  CopyPool() {
+    unsigned hw = std::thread::hardware_concurrency();
+    const int nt = (int)std::min<unsigned>(hw > 1 ? hw - 1 : 0, 15u);
+    for (int i = 0; i < nt; ++i) workers_.emplace_back([this] { loop(); });
+  }
+  ~CopyPool() {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      stop_ = true;
+      ++gen_;
+    }
+    cv_.notify_all();
+    for (auto &t : workers_) t.join();
+  }
+  void loop() {
+    unsigned long long seen = 0;
+    for (;;) {
+      std::unique_lock<std::mutex> lk(mu_);
+      cv_.wait(lk, [&] { return stop_ || gen_ != seen; });
+      if (stop_) return;
+      seen = gen_;
+      lk.unlock();
+      work();
+    }
+  }
+  void work() {
+    for (;;) {
+      int i;
+      const std::function<void(int)> *fn;
+      {
+        std::lock_guard<std::mutex> lk(mu_);
+        if (!fn_ || next_ >= n_) return;
+        i = next_++;
+        fn = fn_;
+      }
+      (*fn)(i);
+      std::lock_guard<std::mutex> lk(mu_);
+      if (++done_ == n_) done_cv_.notify_all();
+    }
+  }
+  std::vector<std::thread> workers_;
+  std::mutex mu_;
+  std::condition_variable cv_, done_cv_;
+  const std::function<void(int)> *fn_ = nullptr;
+  int next_ = 0, n_ = 0, done_ = 0;
+  unsigned long long gen_ = 0;
+  bool stop_ = false;
+};
+
+// memcpy of n bytes split over the pool's threads
+void par_memcpy(void *dst, const void *src, size_t n) {
+  CopyPool &pool = CopyPool::get();
+  const int parts = (int)std::min<size_t>((size_t)pool.threads(), std::max<size_t>(1, n >> 20));
+  const size_t per = (n + parts - 1) / parts;
+  pool.run(parts, [&](int i) {
+    const size_t a = (size_t)i * per;
+    if (a < n) memcpy((char *)dst + a, (const char *)src + a, std::min(per, n - a));
+  });
+}
+
+struct Staging {
+  std::mutex mu;
+  void *buf[2] = {nullptr, nullptr};
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+};
+Staging g_staging;
+
+bool is_pinned(const void *p) {
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return at.type == cudaMemoryTypeHost;
+}
+
+cudaError_t staging_ready() {
+  if (g_staging.buf[0]) return cudaSuccess;
+  for (int k = 0; k < 2; ++k) {
+    cudaError_t e = cudaHostAlloc(&g_staging.buf[k], kChunk, cudaHostAllocDefault);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g_staging.ev[k], cudaEventDisableTiming);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+}  // namespace
+
+cudaError_t copy_host_to_device(void *dst, const void *src, size_t bytes, cudaStream_t st) {
+  if (is_pinned(src)) return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st);
+  std::lock_guard<std::mutex> lk(g_staging.mu);
+  cudaError_t e = staging_ready();
+  if (e != cudaSuccess) return e;
+  size_t off = 0;
+  for (int k = 0; off < bytes; ++k) {
+    const int b = k & 1;
+    const size_t n = std::min(kChunk, bytes - off);
+    // the buffer's previous transfer must have left it before it is refilled
+    if ((e = cudaEventSynchronize(g_staging.ev[b])) != cudaSuccess) return e;
+    par_memcpy(g_staging.buf[b], (const char *)src + off, n);
+    if ((e = cudaMemcpyAsync((char *)dst + off, g_staging.buf[b], n, cudaMemcpyHostToDevice, st)) != cudaSuccess)
+      return e;
+    if ((e = cudaEventRecord(g_staging.ev[b], st)) != cudaSuccess) return e;
+    off += n;
+  }
+  // the staging buffers are shared by all lattices: drain before returning
+  for (int b = 0; b < 2; ++b)
+    if ((e = cudaEventSynchronize(g_staging.ev[b])) != cudaSuccess) return e;
+  return cudaSuccess;
+}
+
+cudaError_t copy_device_to_host(void *dst, const void *src, size_t bytes, cudaStream_t st) {
+  if (is_pinned(dst)) {
+    cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st);
+    return e == cudaSuccess ? cudaStreamSynchronize(st) : e;
+  }
+  std::lock_guard<std::mutex> lk(g_staging.mu);
+  cudaError_t e = staging_ready();
+  if (e != cudaSuccess) return e;
+  const size_t nchunks = (bytes + kChunk - 1) / kChunk;
+  // chunk k goes to buffer k & 1; it is drained to the caller once its copy is
+  // done, while the next chunk's copy runs
+  for (size_t k = 0; k < nchunks + 1; ++k) {
+    if (k < nchunks) {
+      const int b = (int)(k & 1);
+      const size_t off = k * kChunk, n = std::min(kChunk, bytes - off);
+      if ((e = cudaMemcpyAsync(g_staging.buf[b], (const char *)src + off, n, cudaMemcpyDeviceToHost, st)) !=
+          cudaSuccess)
+        return e;
+      if ((e = cudaEventRecord(g_staging.ev[b], st)) != cudaSuccess) return e;
+    }
+    if (k >= 1) {
+      const size_t j = k - 1;
+      const int b = (int)(j & 1);
+      const size_t off = j * kChunk, n = std::min(kChunk, bytes - off);
+      if ((e = cudaEventSynchronize(g_staging.ev[b])) != cudaSuccess) return e;
+      par_memcpy((char *)dst + off, g_staging.buf[b], n);
+    }
+  }
+  return cudaSuccess;
+}
+
+}  // namespace klft

@@ -12,7 +12,12 @@ struct MetroArgs {
   uint64_t seed, chain;
 };
 
+// Launches per sweep: 2 Nd link passes for the SU(3) exp(i eps H) proposal
+// (proposal 1), else the reference's 2^Nd site classes.
+KLFT_HD int metropolis_passes(int nc, int proposal, int nd) { return nc == 3 && proposal == 1 ? 2 * nd : 1 << nd; }
+
 // dtype: 0 = double (plain FP64 form), 1 = float (mixed form)
+// val: the site class, or the link pass 2 mu + parity of the exp proposal
 cudaError_t launch_metropolis_pass(int nc, int dtype, void *links, const Geom &g, int val, const MetroArgs &a,
                                    const uint32_t *d_sweep, unsigned long long *d_nacc, const Defect &df, int block,
                                    cudaStream_t st);

@@ -1,10 +1,12 @@
-// metropolis.cu -- one parity-class pass of the Metropolis sweep on one lattice.
+// metropolis.cu -- one pass of the Metropolis sweep on one lattice.
 //
-// sweep_Metropolis (Metropolis.hpp:118-178) visits the 2^Nd parity classes in
-// the reference's order (class val has parity bit (val >> (Nd-1-d)) & 1 in
-// dimension d, IndexHelper.hpp:84-93); the host enqueues one launch per class.
-// Sites of one class share no staple link, so a pass is race free.  The
-// per-site update is in metropolis_site.cuh.
+// Reference proposals: sweep_Metropolis (Metropolis.hpp:118-178) visits the
+// 2^Nd parity classes in the reference's order (class val has parity bit
+// (val >> (Nd-1-d)) & 1 in dimension d, IndexHelper.hpp:84-93); the host
+// enqueues one launch per class.  Sites of one class share no staple link, so
+// a pass is race free.  exp(i eps H) proposals: 2 Nd link passes (mu, parity)
+// of one thread per link (metropolis_site.cuh).  The per-site and per-link
+// updates are in metropolis_site.cuh.
 #include "metropolis_site.cuh"
 
 namespace klft {
@@ -19,13 +21,14 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::v)
   add_accepts(nacc, d_nacc);
 }
 
+// link pass val = 2 mu + p: U_mu(x) of the V/2 sites of parity p
 template <int ND, typename T, bool DF>
 __global__ void __launch_bounds__(128, MinBlocks<T>::v)
     metropolis_exp_kernel(Links<3, T> U, Geom g, int val, MetroArgs a, const uint32_t *__restrict__ d_sweep,
                           unsigned long long *__restrict__ d_nacc, Defect df) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   int nacc = 0;
-  if (t < g.Vh) nacc = site_update_exp<ND, T, DF>(U, g, pass_site(g, t, val, ND), a, *d_sweep, df);
+  if (t < g.V / 2) nacc = link_update_exp<ND, T, DF>(U, g, link_pass_site(g, t, val & 1, ND), val >> 1, a, *d_sweep, df);
   add_accepts(nacc, d_nacc);
 }
 
@@ -36,7 +39,8 @@ static cudaError_t launch_tdf(const Links<NC, T> &U, const Geom &g, int val, con
   const unsigned grid = (unsigned)((g.Vh + block - 1) / block);
   if constexpr (NC == 3) {
     if (a.proposal == PROPOSAL_EXP) {
-      metropolis_exp_kernel<ND, T, DF><<<grid, block, 0, st>>>(U, g, val, a, d_sweep, d_nacc, df);
+      const unsigned lgrid = (unsigned)((g.V / 2 + block - 1) / block);
+      metropolis_exp_kernel<ND, T, DF><<<lgrid, block, 0, st>>>(U, g, val, a, d_sweep, d_nacc, df);
       return cudaGetLastError();
     }
   }

@@ -10,6 +10,16 @@ autocorrelation model because the chains are independent (each chain's mean
 already averages over its own correlated cycles).
 
     python -m klft_b200.ensemble --L 8 8 8 8 --nc 3 --chains 128 --therm 500 --cycles 20000
+
+`--dS-error` measures instead, on thermalised FP64 SU(3) configurations, the
+error of the mixed form's action change against FP64 hit by hit with
+identical proposals (klft_exp_proposal_dS_error): its mean, spread, largest
+value, its slope against dS (a relative error of beta) and the fraction of hits
+the FP32 accept test decides differently.  These bound the bias of the mixed
+form's stationary plaquette: a relative error k of every dS is a shift of beta
+by beta k, so the plaquette moves by beta k d<P>/d(beta).
+
+    python -m klft_b200.ensemble --dS-error --L 16 16 16 16 --therm 300 --configs 8
 """
 from __future__ import annotations
 
@@ -76,6 +86,33 @@ def compare(L=(8, 8, 8, 8), nc=3, beta=6.0, nhits=10, proposal="exp", eps=0.25, 
     return out
 
 
+def dS_error(L=(16, 16, 16, 16), beta=6.0, nhits=10, eps=0.25, therm=300, configs=8, seed=9100):
+    """Per-hit FP32 vs FP64 action-change error on `configs` configurations of
+    one FP64 chain (hot start, `therm` sweeps, 20 sweeps between configurations)."""
+    g = GaugeField(list(L), 3, "fp64", "hot", seed)
+    g.set_stream(seed, 0)
+    try:
+        g.metropolis(beta, 0.0, nhits, therm, "exp", eps)
+        rows = []
+        for _ in range(configs):
+            g.metropolis(beta, 0.0, nhits, 20, "exp", eps)
+            r = g.exp_dS_error(beta, eps, nhits)
+            r["plaquette"] = g.plaquette()
+            rows.append(r)
+        n = sum(r["hits"] for r in rows)
+        out = {"lattice": list(L), "beta": beta, "eps": eps, "nhits": nhits, "configs": configs, "hits": n,
+               "mean": sum(r["mean"] * r["hits"] for r in rows) / n,
+               "rms": math.sqrt(sum(r["rms"] ** 2 * r["hits"] for r in rows) / n),
+               "max_abs": max(r["max_abs"] for r in rows),
+               "slope": sum(r["slope"] for r in rows) / configs,
+               "slope_spread": float(np.std([r["slope"] for r in rows], ddof=1)) if configs > 1 else None,
+               "decision_flip_fraction": sum(r["decision_flip_fraction"] * r["hits"] for r in rows) / n,
+               "plaquette": float(np.mean([r["plaquette"] for r in rows])), "per_config": rows}
+        return out
+    finally:
+        g.close()
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     ap.add_argument("--L", type=int, nargs="+", default=[8, 8, 8, 8])
@@ -89,7 +126,12 @@ def main(argv=None):
     ap.add_argument("--therm", type=int, default=500)
     ap.add_argument("--cycles", type=int, default=20000)
     ap.add_argument("--seed", type=int, default=9000)
+    ap.add_argument("--dS-error", action="store_true")
+    ap.add_argument("--configs", type=int, default=8)
     a = ap.parse_args(argv)
+    if a.dS_error:
+        print(json.dumps(dS_error(tuple(a.L), a.beta, a.nhits, a.eps, a.therm, a.configs, a.seed)))
+        return
     print(json.dumps(compare(tuple(a.L), a.nc, a.beta, a.nhits, a.proposal, a.eps, a.delta, a.chains, a.therm,
                              a.cycles, a.seed)))
 

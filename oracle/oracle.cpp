@@ -508,66 +508,92 @@ static double wilson_legacy(const Field<NC> &F, int mu, int nu, int Lmu, int Lnu
   return W;
 }
 
-// Metropolis.hpp:73-113 (site functor), :118-178 (sublattice sweep, acceptance norm)
+// One link's hits, Metropolis.hpp:81-107 (reference proposals, U r) or the
+// project's exp(i eps H) proposal (X U, accepted products kept unprojected while
+// the link's hits run and reunitarised once at the end).
+template <int NC>
+static uint64_t link_hits(const Field<NC> &F, long s, int mu, double beta, double delta, int nHits, int proposal,
+                          double eps, Stream &rng, const ExpHit &eh) {
+  const Geo &g = F.g;
+  if (g.open_link(s, mu)) return 0;
+  const bool expprop = NC == 3 && proposal == PROPOSAL_EXP;
+  uint64_t nacc = 0;
+  const Mat<NC> S = staple(F, s, mu);
+  const double c = link_factor(g, F.df, s, mu);
+  Mat<NC> Ucur = F.raw(s, mu);
+  bool changed = false;
+  for (int hit = 0; hit < nHits; ++hit) {
+    const uint32_t h = (uint32_t)(mu * nHits + hit);
+    Mat<NC> r;
+    if constexpr (NC == 3) {
+      if (expprop) r = exp_proposal(eh, h, eps);
+      else randsun(r, rng, delta, proposal, eps);
+    } else {
+      randsun(r, rng, delta, proposal, eps);
+    }
+    // reference proposals U r (Metropolis.hpp:91); exp(i eps H) proposals X U
+    const Mat<NC> Uold = expprop ? Ucur : F.raw(s, mu);
+    const Mat<NC> Unew = expprop ? mul(r, Uold) : mul(Uold, r);
+    double dS = -(beta / (double)NC) * (trace(mul(Unew, S)).real() - trace(mul(Uold, S)).real());
+    if (c != 1.0) dS *= c;
+    bool accept = dS < 0.0;
+    if (!accept) accept = ((expprop ? eh.accept_uniform(h) : rng.drand(0.0, 1.0)) < std::exp(-dS));
+    if (accept) {
+      if (expprop) {
+        Ucur = Unew;
+        changed = true;
+      } else {
+        F.put(s, mu, restore(Unew));
+      }
+      ++nacc;
+    }
+  }
+  if (changed) F.put(s, mu, restore(Ucur));
+  return nacc;
+}
+
+// Metropolis.hpp:73-113 (site functor), :118-178 (sublattice sweep, acceptance
+// norm).  The exp(i eps H) proposal has no reference chain: its sweep is 2 Nd
+// link passes (mu, p), each updating U_mu(x) at every site of parity
+// p = sum_d x_d mod 2 (the links of a pass share no staple link).
 template <int NC>
 static double metropolis_sweep(const Field<NC> &F, double beta, double delta, int nHits, int proposal, double eps,
                                uint64_t seed, uint64_t chain, uint32_t sweep, uint64_t *nacc_out) {
   const Geo &g = F.g;
   const int nd = g.nd;
-  int H[4];
-  long Vh = 1;
-  for (int d = 0; d < 4; ++d) { H[d] = d < nd ? g.L[d] / 2 : 1; Vh *= H[d]; }
   uint64_t nacc = 0;
-  for (int i = 0; i < (1 << nd); ++i) {
-    int bit[4] = {0, 0, 0, 0};
-    for (int k = 0; k < nd; ++k) bit[nd - 1 - k] = (i >> k) & 1;  // IndexHelper.hpp:84-93
-    // sites of one parity class share no staple link and each reads its own
-    // random stream, so the class loop may run on several threads with the
-    // same result (the reference runs it as one parallel_for)
-#pragma omp parallel for schedule(static) reduction(+ : nacc) if (Vh >= 4096)
-    for (long h = 0; h < Vh; ++h) {
-      int x[4] = {0, 0, 0, 0};
-      long t = h;
-      for (int d = 0; d < nd; ++d) { x[d] = 2 * (int)(t % H[d]) + bit[d]; t /= H[d]; }  // IndexHelper.hpp:68-81
-      long s = g.lex(x);
-      Stream rng(seed, chain, (uint32_t)s, sweep, KIND_METROPOLIS, 0);
-      const ExpHit eh(seed, chain, (uint32_t)s, sweep);
-      const bool expprop = NC == 3 && proposal == PROPOSAL_EXP;
-      for (int mu = 0; mu < nd; ++mu) {
-        if (g.open_link(s, mu)) continue;
-        const Mat<NC> S = staple(F, s, mu);
-        const double c = link_factor(g, F.df, s, mu);
-        // exp(i eps H) proposals: accepted products U r are kept unprojected
-        // while the link's hits run and reunitarised once at the end
-        Mat<NC> Ucur = F.raw(s, mu);
-        bool changed = false;
-        for (int hit = 0; hit < nHits; ++hit) {
-          const uint32_t h = (uint32_t)(mu * nHits + hit);
-          Mat<NC> r;
-          if constexpr (NC == 3) {
-            if (expprop) r = exp_proposal(eh, h, eps);
-            else randsun(r, rng, delta, proposal, eps);
-          } else {
-            randsun(r, rng, delta, proposal, eps);
-          }
-          // reference proposals U r (Metropolis.hpp:91); exp(i eps H) proposals X U
-          const Mat<NC> Uold = expprop ? Ucur : F.raw(s, mu);
-          const Mat<NC> Unew = expprop ? mul(r, Uold) : mul(Uold, r);
-          double dS = -(beta / (double)NC) * (trace(mul(Unew, S)).real() - trace(mul(Uold, S)).real());
-          if (c != 1.0) dS *= c;
-          bool accept = dS < 0.0;
-          if (!accept) accept = ((expprop ? eh.accept_uniform(h) : rng.drand(0.0, 1.0)) < std::exp(-dS));
-          if (accept) {
-            if (expprop) {
-              Ucur = Unew;
-              changed = true;
-            } else {
-              F.put(s, mu, restore(Unew));
-            }
-            ++nacc;
-          }
+  if (NC == 3 && proposal == PROPOSAL_EXP) {
+    for (int mu = 0; mu < nd; ++mu)
+      for (int p = 0; p < 2; ++p) {
+#pragma omp parallel for schedule(static) reduction(+ : nacc) if (g.V >= 8192)
+        for (long s = 0; s < g.V; ++s) {
+          int x[4];
+          g.coords(s, x);
+          if (((x[0] + x[1] + x[2] + x[3]) & 1) != p) continue;
+          Stream rng(seed, chain, (uint32_t)s, sweep, KIND_METROPOLIS, 0);
+          const ExpHit eh(seed, chain, (uint32_t)s, sweep);
+          nacc += link_hits(F, s, mu, beta, delta, nHits, proposal, eps, rng, eh);
         }
-        if (changed) F.put(s, mu, restore(Ucur));
+      }
+  } else {
+    int H[4];
+    long Vh = 1;
+    for (int d = 0; d < 4; ++d) { H[d] = d < nd ? g.L[d] / 2 : 1; Vh *= H[d]; }
+    for (int i = 0; i < (1 << nd); ++i) {
+      int bit[4] = {0, 0, 0, 0};
+      for (int k = 0; k < nd; ++k) bit[nd - 1 - k] = (i >> k) & 1;  // IndexHelper.hpp:84-93
+      // sites of one parity class share no staple link and each reads its own
+      // random stream, so the class loop may run on several threads with the
+      // same result (the reference runs it as one parallel_for)
+#pragma omp parallel for schedule(static) reduction(+ : nacc) if (Vh >= 4096)
+      for (long h = 0; h < Vh; ++h) {
+        int x[4] = {0, 0, 0, 0};
+        long t = h;
+        for (int d = 0; d < nd; ++d) { x[d] = 2 * (int)(t % H[d]) + bit[d]; t /= H[d]; }  // IndexHelper.hpp:68-81
+        long s = g.lex(x);
+        Stream rng(seed, chain, (uint32_t)s, sweep, KIND_METROPOLIS, 0);
+        const ExpHit eh(seed, chain, (uint32_t)s, sweep);
+        for (int mu = 0; mu < nd; ++mu) nacc += link_hits(F, s, mu, beta, delta, nHits, proposal, eps, rng, eh);
       }
     }
   }
