@@ -296,23 +296,27 @@ def cpu_baseline_reference(L: int):
 
 # DRAM traffic of one link pass (dram__bytes_read.sum + dram__bytes_write.sum of one
 # metropolis_exp_kernel launch in the ncu capture summarised in the profile below).
-TRAFFIC_PASS_BYTES = None
+TRAFFIC_PASS_BYTES = 204544000 + 17146624
 TRAFFIC_SOURCE = "profiles/metropolis_exp_su3_32x4_mixed.md"
 
 
 def sweep_flops_per_link_update(nhits: int, acceptance: float) -> float:
-    """Algorithmic flops of one SU(3) exp(i eps H) link update (6 per complex
-    multiply, 2 per complex add, 198 per 3x3 product; an FMA counts 2): staple
-    2466, M0 = U0 S 198, per hit the proposal (8 Box-Muller normals 32, the
+    """Flops of one SU(3) exp(i eps H) link update of the mixed form as the
+    kernel forms it (6 per complex multiply, 2 per complex add, 198 per 3x3
+    product, 132 for two rows of one, 42 to complete a third row from the first
+    two; an FMA counts 2): the two-row staple 2574 (per forward term: B's third
+    row 42, C B on two rows 132 and completed 42, A (C B)^+ on two rows 132 and
+    completed 42, the sum 18; per backward term the same with D's and G's third
+    rows), M0 = U0 S 240, per hit the proposal (8 Box-Muller normals 32, the
     Gell-Mann coefficients 8, c1 and c0 = det Q 47, the 12-term coefficient
     series 99, Q^2 from the coefficients 35, X = f0 + f1 Q + f2 Q^2 with its
     hermitian pairs 75) and Re Tr(X A M0) 36, the product X A on every hit but
-    the first (A is the identity there) 198; then the link A U0 198 and one
+    the first (A is the identity there) 198; then the link A U0 240 and one
     reunitarisation (~100).  The accept rate does not enter: the one product
     per hit is also the accepted A."""
     del acceptance
     proposal = 32 + 8 + 47 + 99 + 35 + 75
-    return 2466 + 198 + nhits * (proposal + 36) + (nhits - 1) * 198 + 198 + 100
+    return 2574 + 240 + nhits * (proposal + 36) + (nhits - 1) * 198 + 240 + 100
 
 
 def mixed_errors(g, L):
@@ -416,13 +420,18 @@ def bench_hmc(ntraj: int, cpu: bool = True):
             plaqs.append(g.plaquette())
         dH = np.concatenate(dHs)
         acc = np.concatenate(accs)
-        e = np.exp(np.minimum(-dH, 700.0))
+        # <exp(-dH)> and <dH> over the second half (the first trajectories of the
+        # as-given chain start far from equilibrium with dH of either sign in the
+        # hundreds)
+        h = dH[ntraj // 2:]
+        e = np.exp(-h)
         r = {"trajectories_per_s": ntraj / t_dev, "ms_per_trajectory": t_dev * 1e3 / ntraj,
              "acceptance": float(np.mean(acc != 0)),
              "acceptance_last_half": float(np.mean(acc[ntraj // 2:] != 0)),
-             "mean_exp_mdH": float(np.mean(e)), "mean_exp_mdH_err": float(np.std(e, ddof=1) / np.sqrt(len(e))),
-             "mean_dH": float(np.mean(dH)), "mean_plaquette": float(np.mean(plaqs)),
-             "unitarity": g.unitarity()}
+             "mean_exp_mdH_last_half": float(np.mean(e)),
+             "mean_exp_mdH_last_half_err": float(np.std(e, ddof=1) / np.sqrt(len(e))),
+             "mean_dH_last_half": float(np.mean(h)), "mean_plaquette": float(np.mean(plaqs)),
+             "final_plaquette": plaqs[-1], "unitarity": g.unitarity()}
         g.close()
         return r
 
@@ -468,13 +477,21 @@ def bench_c1(cpu: bool = True):
     U0 = g.download()
     g.set_stream(32091, 0)
 
+    # run_metropolis: sweep `step` then measure when step % 10 == 0 and step != 0,
+    # i.e. after sweeps 11, 21, ..., 991 (99 measurements) of 1000
     def run_gpu():
-        for _ in range(100):
+        g.metropolis(2.0, 0.1, 10, 1)
+        for _ in range(99):
             g.metropolis(2.0, 0.1, 10, 10)
             g.plaquette()
             g.wilson_loop_temporal(C1_TEMPORAL)
             for m, n in C1_PLANES:
                 g.wilson_loop_mu_nu(m, n, C1_PLANAR)
+        g.metropolis(2.0, 0.1, 10, 9)
+
+    def run_fused():
+        return g.run_metropolis_measured(2.0, 0.1, 10, 1000, 10, "reference", 0.0, True, C1_TEMPORAL, C1_PLANES,
+                                         C1_PLANAR)
 
     run_gpu()  # warm-up on a copy of the chain
     g.upload(U0)
@@ -482,10 +499,23 @@ def bench_c1(cpu: bool = True):
     t0 = time.perf_counter()
     run_gpu()
     dt = time.perf_counter() - t0
+    p_calls = g.plaquette()
+    run_fused()  # warm-up
+    g.upload(U0)
+    g.set_counters(0, 0)
+    t0 = time.perf_counter()
+    _, plaq, _, _, dev_ms = run_fused()
+    dt_f = time.perf_counter() - t0
+    p_fused = g.plaquette()
     out = {"workload": "U(1) 4D 8^4, hot start seed 32091, beta 2, delta 0.1, nHits 10, 1000 sweeps, plaquette + "
                        "W_temp (2,2),(3,4),(4,3),(4,4) + W_mu_nu (0,1),(1,2),(3,2) x (2,2),(3,3),(4,3) every 10",
-           "gpu": {"seconds": dt, "link_updates_per_s": 1000 * V * 4 / dt, "plaquette": g.plaquette(),
-                   "path": "GaugeField.metropolis / plaquette / wilson_loop_* (C ABI), FP64, wall clock"}}
+           "gpu_per_call": {"seconds": dt, "link_updates_per_s": 1000 * V * 4 / dt, "plaquette": p_calls,
+                            "path": "GaugeField.metropolis / plaquette / wilson_loop_* per measurement (C ABI), "
+                                    "FP64, wall clock"},
+           "gpu": {"seconds": dt_f, "device_ms": dev_ms, "link_updates_per_s": 1000 * V * 4 / dt_f,
+                   "plaquette": p_fused, "measurements": len(plaq),
+                   "path": "klft_run_metropolis (the run_metropolis loop with its 100 measurements enqueued), "
+                           "FP64, wall clock"}}
     g.close()
     if cpu:
         from oracle.oracle import REF_SO, Lat, RefShim
@@ -496,12 +526,14 @@ def bench_c1(cpu: bool = True):
                 cores = r.set_threads(nt)
                 U = U0.copy()
                 t0 = time.perf_counter()
-                for k in range(100):
-                    r.metropolis(lat, U, 2.0, 0.1, 10, 10, 32091, sweep0=10 * k)
+                r.metropolis(lat, U, 2.0, 0.1, 10, 1, 32091, sweep0=0)
+                for k in range(99):
+                    r.metropolis(lat, U, 2.0, 0.1, 10, 10, 32091, sweep0=1 + 10 * k)
                     r.plaquette(lat, U)
                     r.wilson_temporal(lat, U, C1_TEMPORAL)
                     for m, n in C1_PLANES:
                         r.wilson_mu_nu(lat, U, m, n, C1_PLANAR)
+                r.metropolis(lat, U, 2.0, 0.1, 10, 9, 32091, sweep0=991)
                 dt = time.perf_counter() - t0
                 out[f"cpu_reference_{cores}_threads"] = {
                     "seconds": dt, "link_updates_per_s": 1000 * V * 4 / dt, "plaquette": r.plaquette(lat, U),

@@ -112,6 +112,22 @@ klft_status klft_run_cycles(klft_lattice *lat, double beta, double delta, int nh
                             int ncycles, int measure_plaquette, const int *temporal_pairs, int npairs,
                             double *acc_out, double *plaq_out, double *w_out, double *device_ms);
 
+/* run_metropolis (Metropolis.hpp:180-223) with measureGaugeObservables
+ * (GaugeObservable.hpp:64-127) enqueued on the handle's stream without host
+ * round trips: nsweeps sweeps; after sweep `step` with interval > 0,
+ * step % interval == 0 and step != 0 (so nmeas = (nsweeps - 1) / interval
+ * measurements), the plaquette (when measure_plaquette), WilsonLoop_temporal
+ * over ntemporal (L, T) pairs and WilsonLoop_mu_nu over every (mu, nu) of
+ * `planes` (nplanes (mu, nu) pairs) over nplanar (Lmu, Lnu) pairs.
+ * acc_out[nsweeps], plaq_out[nmeas], wtemp_out[nmeas * ntemporal],
+ * wmunu_out[nmeas * nplanes * nplanar] (plane-major); each may be NULL.
+ * device_ms: CUDA-event time of the whole run. */
+klft_status klft_run_metropolis(klft_lattice *lat, double beta, double delta, int nhits, int proposal, double eps,
+                                int nsweeps, int interval, int measure_plaquette, const int *temporal_pairs,
+                                int ntemporal, const int *planes, int nplanes, const int *planar_pairs, int nplanar,
+                                double *acc_out, double *plaq_out, double *wtemp_out, double *wmunu_out,
+                                double *device_ms);
+
 /* ---------------------------------------------------------------- HMC
  * Conventions of the reference (AdjointGroup.hpp), extended to SU(3) with the
  * Gell-Mann generators t_a: U <- exp(i dt sum_a p_a t_a) U (U(1): e^{i dt p};

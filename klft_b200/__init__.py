@@ -192,6 +192,33 @@ class GaugeField:
                                     C.byref(ms)))
         return acc[:ncycles], plaq[:ncycles], w[:ncycles, :len(p)], ms.value
 
+    def run_metropolis_measured(self, beta: float, delta: float, nhits: int, nsweeps: int, interval: int,
+                                proposal: str = "reference", eps: float = 0.0, measure_plaquette: bool = True,
+                                temporal_pairs=(), planes=(), planar_pairs=()):
+        """klft_run_metropolis: nsweeps sweeps with measurements after sweeps
+        interval, 2 interval, ... < nsweeps, all enqueued without host round
+        trips.  Returns (acc[nsweeps], plaq[nmeas], W_temp[nmeas, ntemporal],
+        W_mu_nu[nmeas, nplanes, nplanar], device_ms)."""
+        tp = _pairs(temporal_pairs) if len(temporal_pairs) else np.zeros((0, 2), dtype=np.int32)
+        pl = _pairs(planes) if len(planes) else np.zeros((0, 2), dtype=np.int32)
+        pp = _pairs(planar_pairs) if len(planar_pairs) else np.zeros((0, 2), dtype=np.int32)
+        nmeas = (nsweeps - 1) // interval if interval > 0 and nsweeps > 0 else 0
+        acc = np.zeros(max(nsweeps, 1))
+        plaq = np.zeros(max(nmeas, 1))
+        wt = np.zeros((max(nmeas, 1), max(len(tp), 1)))
+        wm = np.zeros((max(nmeas, 1), max(len(pl), 1), max(len(pp), 1)))
+        ms = C.c_double()
+        dp = C.POINTER(C.c_double)
+        ip = C.POINTER(C.c_int)
+        check(lib().klft_run_metropolis(self._h, beta, delta, nhits, PROPOSAL[proposal], eps, nsweeps, interval,
+                                        int(measure_plaquette), tp.ctypes.data_as(ip), len(tp), pl.ctypes.data_as(ip),
+                                        len(pl), pp.ctypes.data_as(ip), len(pp), acc.ctypes.data_as(dp),
+                                        plaq.ctypes.data_as(dp), wt.ctypes.data_as(dp), wm.ctypes.data_as(dp),
+                                        C.byref(ms)))
+        wt = wt[:nmeas, :len(tp)]
+        wm = wm.reshape(max(nmeas, 1), -1)[:nmeas, :len(pl) * len(pp)].reshape(nmeas, len(pl), len(pp))
+        return acc[:nsweeps], plaq[:nmeas], wt, wm, ms.value
+
     # -- HMC
     def ncomp(self) -> int:
         return {1: 1, 2: 3, 3: 8}[self.nc]
@@ -478,8 +505,32 @@ def flushAllGaugeObservables(params: GaugeObservableParams, header: bool = True)
 
 
 def run_metropolis(g: GaugeField, mp: MetropolisParams, op: GaugeObservableParams, verbosity: int = 0) -> int:
-    """Metropolis.hpp:180-223."""
+    """Metropolis.hpp:180-223.  Without per-step output (verbosity 0) the whole
+    run is one klft_run_metropolis call; the measurements are the same."""
     import time
+    if verbosity == 0:
+        tp = op.W_temp_L_T_pairs if op.measure_wilson_loop_temporal else []
+        pl = op.W_mu_nu_pairs if op.measure_wilson_loop_mu_nu else []
+        pp = op.W_Lmu_Lnu_pairs if op.measure_wilson_loop_mu_nu else []
+        _, plaq, wt, wm, _ = g.run_metropolis_measured(mp.beta, mp.delta, mp.nHits, mp.nSweep,
+                                                       op.measurement_interval, mp.proposal, mp.eps,
+                                                       op.measure_plaquette, tp, pl, pp)
+        for i in range(len(plaq) if op.measurement_interval else 0):
+            step = (i + 1) * op.measurement_interval
+            if op.measure_plaquette:
+                op.plaquette_measurements.append(float(plaq[i]))
+            if op.measure_wilson_loop_temporal:
+                op.W_temp_measurements.append([(float(p[0]), float(p[1]), float(x))
+                                               for p, x in zip(_pairs(tp), wt[i])])
+            if op.measure_wilson_loop_mu_nu:
+                rows = []
+                for q, (mu, nu) in enumerate(_pairs(pl)):
+                    rows += [(float(mu), float(nu), float(p[0]), float(p[1]), float(x))
+                             for p, x in zip(_pairs(pp), wm[i, q])]
+                op.W_mu_nu_measurements.append(rows)
+            op.measurement_steps.append(step)
+        flushAllGaugeObservables(op)
+        return 0
     for step in range(mp.nSweep):
         t0 = time.perf_counter()
         acc = sweep_Metropolis(g, mp)

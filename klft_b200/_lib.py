@@ -73,6 +73,8 @@ SIGNATURES = {
     "klft_run_cycles": (C.c_int, [_vp, C.c_double, C.c_double, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, _ip,
                                   C.c_int, _dp, _dp, _dp, _dp]),
     "klft_peak_flops": (C.c_int, [C.c_int, _dp]),
+    "klft_run_metropolis": (C.c_int, [_vp, C.c_double, C.c_double, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int,
+                                      C.c_int, _ip, C.c_int, _ip, C.c_int, _ip, C.c_int, _dp, _dp, _dp, _dp, _dp]),
     "klft_exp_proposal_dS_error": (C.c_int, [_vp, C.c_double, C.c_double, C.c_int, _dp]),
     "klft_hmc_trajectories": (C.c_int, [_vp, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, _dp, _ip]),
     "klft_hmc_integrate": (C.c_int, [_vp, C.c_double, C.c_double, C.c_int, C.c_int]),

@@ -70,8 +70,9 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::v)
   int nacc = 0;
   const Links<NC, T> U{(cx<T> *)c.links, c.g.V};
   if constexpr (EXP && NC == 3) {
-    if (t < c.g.V / 2)
-      nacc = link_update_exp<ND, T, DF>(U, c.g, link_pass_site(c.g, t, val & 1, ND), val >> 1, c.a, *c.ctr, c.df);
+    bool ok = false;
+    const Site x = link_pass_site(c.g, t, val & 1, ND, ok);
+    if (ok && t < link_pass_threads(c.g, ND)) nacc = link_update_exp<ND, T, DF>(U, c.g, x, val >> 1, c.a, *c.ctr, c.df);
   } else {
     if (t < c.g.Vh) nacc = site_update_ref<NC, ND, T, DF>(U, c.g, pass_site(c.g, t, val, ND), c.a, *c.ctr, c.df);
   }
@@ -379,7 +380,7 @@ klft_status enqueue_multi_sweep(const std::vector<SweepItem> &items, unsigned lo
     d.index = it.acc_index >= 0 ? it.acc_index : i;
     d.block_begin = grp->blocks.back();
     // exp groups: V/2 links per link pass; reference groups: Vh sites per class
-    const long long nthr = key.exp ? lat->g.V / 2 : lat->g.Vh;
+    const long long nthr = key.exp ? link_pass_threads(lat->g, lat->g.nd) : lat->g.Vh;
     grp->blocks.back() += (int)((nthr + block - 1) / block);
   }
   int maxpass = 0;

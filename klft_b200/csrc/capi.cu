@@ -539,6 +539,125 @@ klft_status klft_run_cycles(klft_lattice *lat, double beta, double delta, int nh
   return KLFT_OK;
 }
 
+klft_status klft_run_metropolis(klft_lattice *lat, double beta, double delta, int nhits, int proposal, double eps,
+                                int nsweeps, int interval, int measure_plaquette, const int *temporal_pairs,
+                                int ntemporal, const int *planes, int nplanes, const int *planar_pairs, int nplanar,
+                                double *acc_out, double *plaq_out, double *wtemp_out, double *wmunu_out,
+                                double *device_ms) {
+  const char *who = "klft_run_metropolis";
+  if (!lat) return fail(KLFT_EINVAL, "%s: null handle", who);
+  if (nsweeps < 0 || nhits < 0 || interval < 0 || ntemporal < 0 || nplanes < 0 || nplanar < 0)
+    return fail(KLFT_EINVAL, "%s: negative count", who);
+  if ((ntemporal > 0 && !temporal_pairs) || (nplanes > 0 && !planes) || (nplanar > 0 && !planar_pairs))
+    return fail(KLFT_EINVAL, "%s: null list", who);
+  klft_status v = check_proposal(lat, delta, proposal, eps, who);
+  if (v != KLFT_OK) return v;
+  const int nd = lat->g.nd;
+  for (int k = 0; k < ntemporal; ++k)
+    if (temporal_pairs[2 * k] < 0 || temporal_pairs[2 * k + 1] < 0)
+      return fail(KLFT_EINVAL, "%s: negative loop extent", who);
+  for (int k = 0; k < nplanar; ++k)
+    if (planar_pairs[2 * k] < 0 || planar_pairs[2 * k + 1] < 0) return fail(KLFT_EINVAL, "%s: negative loop extent", who);
+  for (int q = 0; q < nplanes; ++q) {
+    const int mu = planes[2 * q], nu = planes[2 * q + 1];
+    if (mu < 0 || nu < 0 || mu >= nd || nu >= nd || mu == nu) return fail(KLFT_EINVAL, "%s: bad plane (%d, %d)", who, mu, nu);
+  }
+  if (nsweeps == 0) return KLFT_OK;
+  LOCK(lat);
+  // measurements after sweeps step = interval, 2 interval, ... < nsweeps (GaugeObservable.hpp:69-73)
+  const int nmeas = interval > 0 ? (nsweeps - 1) / interval : 0;
+  const bool do_plaq = measure_plaquette && nmeas > 0;
+  const int ntw = ntemporal > 0 && nmeas > 0 ? (nd - 1) * ntemporal : 0;  // sums per measurement
+  const int npw = nplanar > 0 && nmeas > 0 ? nplanes * nplanar : 0;
+  const size_t per = 1 + (size_t)ntw + (size_t)npw;
+  CK(lat->s_aux.ensure((size_t)nsweeps * sizeof(unsigned long long)));
+  CK(lat->s_wl.ensure(((size_t)nmeas * per + 1) * sizeof(double)));
+  unsigned long long *d_nacc = (unsigned long long *)lat->s_aux.ptr;
+  double *d_res = (double *)lat->s_wl.ptr;
+  // plans: temporal loops along nu = Nd-1, one plan per distinct nu of the planar list
+  CK(lat->s_tab.ensure((2 * (size_t)ntemporal + (size_t)nplanes * 2 * nplanar) * sizeof(int) + 16));
+  WilsonPlan tplan;
+  size_t toff = 0;
+  if (ntw > 0) {
+    klft_status s = make_wilson_plan(lat, temporal_pairs, ntemporal, nd - 1, tplan, toff);
+    if (s != KLFT_OK) return s;
+    toff += 2 * (size_t)ntemporal;
+  }
+  std::vector<WilsonPlan> pplan(npw > 0 ? nplanes : 0);
+  for (int q = 0; q < (int)pplan.size(); ++q) {
+    klft_status s = make_wilson_plan(lat, planar_pairs, nplanar, planes[2 * q + 1], pplan[q], toff);
+    if (s != KLFT_OK) return s;
+    toff += 2 * (size_t)nplanar;
+  }
+  {
+    const int nblk = plaquette_blocks(lat->g);
+    if (lat->s_part.cap < (size_t)nblk * sizeof(double)) CK(lat->s_part.ensure((size_t)nblk * sizeof(double)));
+  }
+  CK(cudaMemsetAsync(d_nacc, 0, (size_t)nsweeps * sizeof(unsigned long long), lat->stream));
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  CK(cudaEventRecord(e0, lat->stream));
+  int m = 0;
+  for (int step = 0; step < nsweeps; ++step) {
+    klft_status s = enqueue_sweeps(lat, beta, delta, nhits, proposal, eps, 1, d_nacc + step, lat->defect);
+    if (s != KLFT_OK) return s;
+    if (!(interval > 0 && step % interval == 0 && step != 0)) continue;
+    double *slot = d_res + (size_t)m * per;
+    if (do_plaq)
+      CK(launch_plaquette(lat->nc, lat->dtype(), lat->links, lat->g, (double *)lat->s_part.ptr,
+                          plaquette_blocks(lat->g), slot, lat->stream));
+    int last_nu = -1;
+    for (int mu = 0; mu < nd - 1 && ntw > 0; ++mu) {
+      s = enqueue_wilson_plane(lat, tplan, mu, nd - 1, last_nu == nd - 1, slot + 1 + (size_t)mu * ntemporal);
+      if (s != KLFT_OK) return s;
+      last_nu = nd - 1;
+    }
+    for (int q = 0; q < (int)pplan.size(); ++q) {
+      const int mu = planes[2 * q], nu = planes[2 * q + 1];
+      s = enqueue_wilson_plane(lat, pplan[q], mu, nu, last_nu == nu, slot + 1 + ntw + (size_t)q * nplanar);
+      if (s != KLFT_OK) return s;
+      last_nu = nu;
+    }
+    ++m;
+  }
+  CK(cudaEventRecord(e1, lat->stream));
+  std::vector<unsigned long long> h_nacc(nsweeps);
+  std::vector<double> h_res((size_t)nmeas * per);
+  CK(cudaMemcpyAsync(h_nacc.data(), d_nacc, (size_t)nsweeps * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                     lat->stream));
+  if (!h_res.empty())
+    CK(cudaMemcpyAsync(h_res.data(), d_res, h_res.size() * sizeof(double), cudaMemcpyDeviceToHost, lat->stream));
+  CK(cudaStreamSynchronize(lat->stream));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (device_ms) *device_ms = ms;
+  double norm = 1.0;
+  for (int d = 0; d < nd; ++d) norm *= (double)lat->g.L[d];
+  norm *= (double)nd * (double)nhits;
+  for (int k = 0; k < nsweeps; ++k)
+    if (acc_out) acc_out[k] = nhits > 0 ? (double)h_nacc[k] / norm : 0.0;
+  for (int i = 0; i < nmeas; ++i) {
+    const double *r = h_res.data() + (size_t)i * per;
+    if (plaq_out && do_plaq) plaq_out[i] = normalize_plaquette(lat, r[0]);
+    if (wtemp_out)
+      for (int k = 0; k < ntemporal && ntw > 0; ++k) {
+        // WilsonLoop.hpp:250-304: the average over the spatial directions mu
+        double acc = 0.0;
+        for (int mu = 0; mu < nd - 1; ++mu) {
+          const double w = normalize_wilson(lat, r[1 + (size_t)mu * ntemporal + k]);
+          acc = mu == 0 ? w : acc + w;
+        }
+        wtemp_out[(size_t)i * ntemporal + k] = acc / (double)(nd - 1);
+      }
+    if (wmunu_out)
+      for (int j = 0; j < npw; ++j) wmunu_out[(size_t)i * npw + j] = normalize_wilson(lat, r[1 + ntw + j]);
+  }
+  return KLFT_OK;
+}
+
 }  // extern "C"
 
 // ------------------------------------------------------------------ enqueue helpers
@@ -611,9 +730,11 @@ double normalize_wilson(const klft_lattice *lat, double sum) {
 // Build the device tables for a pair list: the pairs themselves (direct form)
 // and, for the gauge-fixed form, the (T, pair) lists per loop length L.  All
 // scratch the plane kernels need is sized here, before anything is enqueued.
-klft_status make_wilson_plan(klft_lattice *lat, const int *pairs, int npairs, int nu, WilsonPlan &plan) {
+klft_status make_wilson_plan(klft_lattice *lat, const int *pairs, int npairs, int nu, WilsonPlan &plan,
+                             size_t tab_off) {
   plan = WilsonPlan();
   plan.npairs = npairs;
+  plan.tab_off = tab_off;
   bool degenerate = false;
   for (int k = 0; k < npairs; ++k) {
     plan.lmax = pairs[2 * k] > plan.lmax ? pairs[2 * k] : plan.lmax;
@@ -637,8 +758,9 @@ klft_status make_wilson_plan(klft_lattice *lat, const int *pairs, int npairs, in
     plan.off[plan.lmax + 1] = (int)plan.T.size();
     CK(lat->s_gf.ensure(wilson_gf_scratch(lat->nc, lat->dtype(), lat->g, nu, plan.tmax)));
   }
-  CK(lat->s_tab.ensure(h.size() * sizeof(int) + 16));
-  CK(cudaMemcpyAsync(lat->s_tab.ptr, h.data(), h.size() * sizeof(int), cudaMemcpyHostToDevice, lat->stream));
+  CK(lat->s_tab.ensure((tab_off + h.size()) * sizeof(int) + 16));
+  CK(cudaMemcpyAsync((int *)lat->s_tab.ptr + tab_off, h.data(), h.size() * sizeof(int), cudaMemcpyHostToDevice,
+                     lat->stream));
   CK(cudaStreamSynchronize(lat->stream));  // h is pageable and local
   const int nblk = plan.gf ? wilson_gf_blocks(lat->g) : plaquette_blocks(lat->g);
   CK(lat->s_part.ensure((size_t)nblk * (npairs > 1 ? npairs : 1) * sizeof(double)));
@@ -648,7 +770,7 @@ klft_status make_wilson_plan(klft_lattice *lat, const int *pairs, int npairs, in
 // enqueue: d_out[k] = unnormalised sum over sites of Re Tr W for pair k of the plan
 klft_status enqueue_wilson_plane(klft_lattice *lat, const WilsonPlan &plan, int mu, int nu, bool omega_ready,
                                  double *d_out) {
-  const int *tab = (const int *)lat->s_tab.ptr;
+  const int *tab = (const int *)lat->s_tab.ptr + plan.tab_off;
   if (plan.gf) {
     const int *ht[3] = {plan.off.data(), plan.T.data(), plan.p.data()};
     CK(launch_wilson_gf(lat->nc, lat->dtype(), lat->links, lat->g, mu, nu, ht, plan.lmax, plan.tmax, plan.npairs,

@@ -117,10 +117,14 @@ size_t hmc_footprint(int nc, int dtype, const Geom &g, int ntraj);
 struct WilsonPlan {
   int npairs = 0, lmax = 0, tmax = 0;
   bool gf = false;
+  size_t tab_off = 0;  // the pairs' position (ints) in the handle's device table
   // gauge-fixed form: loops of length L are entries off[L] .. off[L+1]-1 of (T, pair)
   std::vector<int> off, T, p;
 };
-klft_status make_wilson_plan(klft_lattice *lat, const int *pairs, int npairs, int nu, WilsonPlan &plan);
+// tab_off: where the pairs go in lat->s_tab (several plans in flight at once
+// use disjoint ranges; the caller then sizes s_tab for all of them first)
+klft_status make_wilson_plan(klft_lattice *lat, const int *pairs, int npairs, int nu, WilsonPlan &plan,
+                             size_t tab_off = 0);
 klft_status enqueue_wilson_plane(klft_lattice *lat, const WilsonPlan &plan, int mu, int nu, bool omega_ready,
                                  double *d_out);
 klft_status wilson_sums(klft_lattice *lat, int mu, int nu, const int *pairs, int npairs, double *sums);

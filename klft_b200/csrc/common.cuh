@@ -399,6 +399,16 @@ template <int N, typename T> struct Links {
     }
     return m;
   }
+  // rows 0 and 1 only (row 2 left unset), for callers that never read it
+  KLFT_D Mat<N, T> load_rows01(long long lin, int mu) const {
+    Mat<N, T> m;
+    const cx<T> *q = p + (long long)mu * P * V + lin;
+#pragma unroll
+    for (int i = 0; i < (N < 2 ? N : 2); ++i)
+#pragma unroll
+      for (int j = 0; j < N; ++j) m.e[i][j] = q[(i * N + j) * V];
+    return m;
+  }
   KLFT_D void store(long long lin, int mu, const Mat<N, T> &m) const {
     cx<T> *q = p + (long long)mu * P * V + lin;
 #pragma unroll

@@ -28,7 +28,9 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::v)
                           unsigned long long *__restrict__ d_nacc, Defect df) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   int nacc = 0;
-  if (t < g.V / 2) nacc = link_update_exp<ND, T, DF>(U, g, link_pass_site(g, t, val & 1, ND), val >> 1, a, *d_sweep, df);
+  bool ok = false;
+  const Site x = link_pass_site(g, t, val & 1, ND, ok);
+  if (ok && t < link_pass_threads(g, ND)) nacc = link_update_exp<ND, T, DF>(U, g, x, val >> 1, a, *d_sweep, df);
   add_accepts(nacc, d_nacc);
 }
 
@@ -39,7 +41,7 @@ static cudaError_t launch_tdf(const Links<NC, T> &U, const Geom &g, int val, con
   const unsigned grid = (unsigned)((g.Vh + block - 1) / block);
   if constexpr (NC == 3) {
     if (a.proposal == PROPOSAL_EXP) {
-      const unsigned lgrid = (unsigned)((g.V / 2 + block - 1) / block);
+      const unsigned lgrid = (unsigned)((link_pass_threads(g, ND) + block - 1) / block);
       metropolis_exp_kernel<ND, T, DF><<<lgrid, block, 0, st>>>(U, g, val, a, d_sweep, d_nacc, df);
       return cudaGetLastError();
     }

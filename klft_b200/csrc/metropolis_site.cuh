@@ -153,12 +153,24 @@ KLFT_D int site_update_ref(const Links<NC, T> &U, const Geom &g, const Site &x, 
 // (the reference-proposal update keeps one thread per site of a class and the
 // reference's order, for hit-by-hit parity with klft).
 
-// Site t of the sites of parity p (t < V/2): class c = t / Vh among the
-// 2^(Nd-1) site classes of that parity, class bits sub = (c << 1) | b0 with b0
-// fixing the parity, hidx = t mod Vh.
-KLFT_D Site link_pass_site(const Geom &g, long long t, int p, int nd) {
-  const unsigned c = (unsigned)(t / g.Vh);
-  unsigned hidx = (unsigned)(t - (long long)c * g.Vh);
+// Site t of the sites of parity p.  Within a pass the threads run over chunks
+// of 32 consecutive half-lattice indices hidx, and within a chunk over the
+// 2^(Nd-1) site classes of that parity (class c: bits sub = (c << 1) | b0, b0
+// fixing the parity): a warp reads 32 consecutive sites of one class
+// (coalesced), and the warps in flight at any time share one small hidx window,
+// so the staple neighbourhoods they read are reused from L2.  Threads
+// t < link_pass_threads(g, nd) cover the V/2 sites once; those with hidx >= Vh
+// (Vh not a multiple of 32) have no site (ok = false).
+KLFT_HD long long link_pass_threads(const Geom &g, int nd) {
+  return (g.Vh + 31) / 32 * 32 * (1ll << (nd - 1));
+}
+KLFT_D Site link_pass_site(const Geom &g, long long t, int p, int nd, bool &ok) {
+  const unsigned ncls = 1u << (nd - 1);
+  const unsigned lane = (unsigned)(t & 31);
+  const unsigned long long w = (unsigned long long)(t >> 5);
+  const unsigned c = (unsigned)(w % ncls);
+  unsigned hidx = (unsigned)((w / ncls) * 32u + lane);
+  ok = hidx < (unsigned)g.Vh;
   const unsigned sub = (c << 1) | ((unsigned)(__popc(c) & 1) ^ (unsigned)p);
   Site x;
 #pragma unroll
@@ -203,7 +215,10 @@ KLFT_D int link_update_exp(const Links<3, T> &U, const Geom &g, const Site &x, i
   const T cdef = DF && df.active && in_defect(g, df, x, mu) ? (T)defect_c(df) : T(1);
   // M0 = U0 S stays fixed; A is the product of the accepted X, so the current
   // link is A U0 and Re Tr(X A U0 S) = Re Tr((X A) M0): one product X A per hit
-  const Mat<3, T> M0 = mul(U.load(lx, mu), staple<3, ND, T, DF>(U, g, x, mu, df));
+  Mat<3, T> S;
+  if constexpr (sizeof(T) == 4 && !DF) S = staple_su3_2row<ND>(U, g, x, mu);
+  else S = staple<3, ND, T, DF>(U, g, x, mu, df);
+  const Mat<3, T> M0 = mul(U.load(lx, mu), S);
   Mat<3, T> A = mident<3, T>();
   T trO = retr_diag(M0);
   uint32_t aw[4];

@@ -42,6 +42,73 @@ KLFT_D Mat<NC, T> staple(const Links<NC, T> &U, const Geom &g, const Site &x, in
   return S;
 }
 
+// SU(3) with links stored as two FP32 rows (the mixed form, no defect): every
+// staple term is a product of three SU(3) links and so itself in SU(3), which
+// lets most of its third rows come from the first two (row 2 = conj(row 0 x
+// row 1)) instead of from products:
+//   forward  A B^+ C^+ = A (C B)^+,  backward  D^+ E^+ G = (E D)^+ G,
+// with C B and E D formed on their first two rows (C and E need no third row),
+// completed, and each term formed on its first two rows and completed.  Same
+// terms in the same order as staple(); rounding differs at FP32 level.
+template <typename T> KLFT_D void complete_row2(Mat<3, T> &m) {
+  m.e[2][0] = conj(m.e[0][1] * m.e[1][2] - m.e[0][2] * m.e[1][1]);
+  m.e[2][1] = conj(m.e[0][2] * m.e[1][0] - m.e[0][0] * m.e[1][2]);
+  m.e[2][2] = conj(m.e[0][0] * m.e[1][1] - m.e[0][1] * m.e[1][0]);
+}
+// rows 0, 1 of a b (a's third row is not read)
+template <typename T> KLFT_D void mul_rows01(const Mat<3, T> &a, const Mat<3, T> &b, Mat<3, T> &c) {
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) c.e[i][j] = a.e[i][0] * b.e[0][j] + a.e[i][1] * b.e[1][j] + a.e[i][2] * b.e[2][j];
+}
+// rows 0, 1 of a b^+
+template <typename T> KLFT_D void mul_nd_rows01(const Mat<3, T> &a, const Mat<3, T> &b, Mat<3, T> &c) {
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+      c.e[i][j] = a.e[i][0] * conj(b.e[j][0]) + a.e[i][1] * conj(b.e[j][1]) + a.e[i][2] * conj(b.e[j][2]);
+}
+// rows 0, 1 of a^+ b
+template <typename T> KLFT_D void mul_dn_rows01(const Mat<3, T> &a, const Mat<3, T> &b, Mat<3, T> &c) {
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+      c.e[i][j] = conj(a.e[0][i]) * b.e[0][j] + conj(a.e[1][i]) * b.e[1][j] + conj(a.e[2][i]) * b.e[2][j];
+}
+
+template <int ND>
+KLFT_D Mat<3, float> staple_su3_2row(const Links<3, float> &U, const Geom &g, const Site &x, int mu) {
+  Mat<3, float> S = mzero<3, float>();
+  const Site xpmu = site_up(g, x, mu);
+#pragma unroll 1
+  for (int nu = 0; nu < ND; ++nu) {
+    if (nu == mu) continue;
+    const Site xpnu = site_up(g, x, nu);
+    Mat<3, float> cb, f;
+    mul_rows01(U.load_rows01(site_lin(g, x), nu), U.load(site_lin(g, xpnu), mu), cb);
+    complete_row2(cb);
+    mul_nd_rows01(U.load_rows01(site_lin(g, xpmu), nu), cb, f);
+    complete_row2(f);
+    madd(S, f);
+  }
+#pragma unroll 1
+  for (int nu = 0; nu < ND; ++nu) {
+    if (nu == mu) continue;
+    const Site xpmu_mnu = site_dn(g, xpmu, nu);
+    const Site xmnu = site_dn(g, x, nu);
+    Mat<3, float> ed, f;
+    mul_rows01(U.load_rows01(site_lin(g, xmnu), mu), U.load(site_lin(g, xpmu_mnu), nu), ed);
+    complete_row2(ed);
+    mul_dn_rows01(ed, U.load(site_lin(g, xmnu), nu), f);
+    complete_row2(f);
+    madd(S, f);
+  }
+  return S;
+}
+
 // The same staple with mu fixed at compile time and the nu loops unrolled: the
 // same products in the same order, but every site step and index folds to a few
 // integer operations.  For kernels without proposal code (the HMC force), where

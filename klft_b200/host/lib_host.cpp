@@ -331,7 +331,50 @@ void clearAllGaugeObservables(GaugeObservableParams &p) {
 }
 
 // Metropolis.hpp:180-223
+// Without per-step output the whole loop is one klft_run_metropolis call (the
+// same sweeps and measurements, no host round trip per step).
+static int run_metropolis_fused(klft_lattice *g, const MetropolisParams &mp, GaugeObservableParams &op) {
+  std::vector<int> tp, pl, pp;
+  if (op.measure_wilson_loop_temporal)
+    for (const auto &q : op.W_temp_L_T_pairs) { tp.push_back(q[0]); tp.push_back(q[1]); }
+  if (op.measure_wilson_loop_mu_nu) {
+    for (const auto &q : op.W_mu_nu_pairs) { pl.push_back(q[0]); pl.push_back(q[1]); }
+    for (const auto &q : op.W_Lmu_Lnu_pairs) { pp.push_back(q[0]); pp.push_back(q[1]); }
+  }
+  const int nsweeps = (int)mp.nSweep, interval = (int)op.measurement_interval;
+  const int nmeas = interval > 0 && nsweeps > 0 ? (nsweeps - 1) / interval : 0;
+  const int ntp = (int)tp.size() / 2, npl = (int)pl.size() / 2, npp = (int)pp.size() / 2;
+  std::vector<double> plaq(nmeas > 0 ? nmeas : 1), wt((size_t)(nmeas > 0 ? nmeas : 1) * (ntp > 0 ? ntp : 1)),
+      wm((size_t)(nmeas > 0 ? nmeas : 1) * (npl * npp > 0 ? npl * npp : 1));
+  if (klft_run_metropolis(g, mp.beta, mp.delta, (int)mp.nHits, mp.proposal, mp.eps, nsweeps, interval,
+                          op.measure_plaquette ? 1 : 0, tp.data(), ntp, pl.data(), npl, pp.data(), npp, nullptr,
+                          plaq.data(), wt.data(), wm.data(), nullptr) != KLFT_OK) {
+    printf("Error: %s\n", klft_last_error());
+    return -1;
+  }
+  for (int i = 0; i < nmeas; ++i) {
+    if (op.measure_plaquette) op.plaquette_measurements.push_back(plaq[i]);
+    if (op.measure_wilson_loop_temporal) {
+      std::vector<std::array<real_t, 3>> rows;
+      for (int k = 0; k < ntp; ++k) rows.push_back({(real_t)tp[2 * k], (real_t)tp[2 * k + 1], wt[(size_t)i * ntp + k]});
+      op.W_temp_measurements.push_back(rows);
+    }
+    if (op.measure_wilson_loop_mu_nu) {
+      std::vector<std::array<real_t, 5>> rows;
+      for (int q = 0; q < npl; ++q)
+        for (int k = 0; k < npp; ++k)
+          rows.push_back({(real_t)pl[2 * q], (real_t)pl[2 * q + 1], (real_t)pp[2 * k], (real_t)pp[2 * k + 1],
+                          wm[((size_t)i * npl + q) * npp + k]});
+      op.W_mu_nu_measurements.push_back(rows);
+    }
+    op.measurement_steps.push_back((size_t)(i + 1) * op.measurement_interval);
+  }
+  flushAllGaugeObservables(op);
+  return 0;
+}
+
 int run_metropolis(klft_lattice *g, const MetropolisParams &mp, GaugeObservableParams &op) {
+  if (g_verbosity == 0) return run_metropolis_fused(g, mp, op);
   for (size_t step = 0; step < (size_t)mp.nSweep; ++step) {
     const auto t0 = std::chrono::steady_clock::now();
     const real_t acc_rate = sweep_Metropolis(g, mp);

@@ -28,3 +28,37 @@ def test_cycles_match_single_calls(L, nc, pairs, precision, rtol, atol):
         assert plaq[c] == pytest.approx(b.plaquette(), rel=rtol, abs=atol)
         np.testing.assert_allclose(w[c], b.wilson_loop_temporal(pairs), rtol=rtol, atol=atol)
     np.testing.assert_array_equal(a.download(), b.download())
+
+
+@pytest.mark.parametrize("L,nc,precision", [([8, 8, 8, 8], 1, "fp64"), ([4, 4, 6, 4], 3, "mixed"),
+                                            ([6, 4, 8], 2, "fp64"), ([8, 6], 3, "fp64")])
+def test_run_metropolis_fused_matches_single_calls(L, nc, precision):
+    """klft_run_metropolis (measurements every `interval` sweeps, step 0
+    excluded, temporal and planar loops, all enqueued) against the same run
+    through the single-call API, measurement by measurement, bit for bit."""
+    beta = {1: 2.0, 2: 2.3, 3: 6.0}[nc]
+    prop = "exp" if nc == 3 else "reference"
+    nd = len(L)
+    tp = [(1, 1), (2, 2), (2, 1)]
+    planes = [(0, 1), (1, 0)] + ([(1, 2), (2, 0)] if nd > 2 else [])
+    pp = [(1, 1), (2, 2), (2, 1)]
+    a = GaugeField(L, nc, precision, "hot", 32091)
+    b = GaugeField(L, nc, precision, "hot", 32091)
+    a.set_stream(32091, 1)
+    b.set_stream(32091, 1)
+    nsweeps, interval = 23, 5
+    acc, plaq, wt, wm, ms = a.run_metropolis_measured(beta, 0.1, 4, nsweeps, interval, prop, 0.25, True, tp, planes,
+                                                      pp)
+    assert ms > 0 and len(plaq) == (nsweeps - 1) // interval == wt.shape[0] == wm.shape[0]
+    m = 0
+    for step in range(nsweeps):
+        assert acc[step] == b.metropolis(beta, 0.1, 4, 1, prop, 0.25)[0]
+        if step % interval == 0 and step != 0:
+            assert plaq[m] == b.plaquette()
+            np.testing.assert_array_equal(wt[m], b.wilson_loop_temporal(tp))
+            for q, (mu, nu) in enumerate(planes):
+                np.testing.assert_array_equal(wm[m, q], b.wilson_loop_mu_nu(mu, nu, pp))
+            m += 1
+    np.testing.assert_array_equal(a.download(), b.download())
+    a.close()
+    b.close()
