@@ -197,17 +197,27 @@ def kernel_split(g, eps, reps=3):
     return ms_sweep / reps, max(ms_all - ms_sweep, 0.0) / reps
 
 
-def e2e_public_api(g, eps, steps):
-    """Per step through the public API with host buffers: sweep, plaquette, W_temp."""
+def e2e_public_api(g, eps, steps, per_call=False):
+    """Per step through the public API with host buffers: one klft_run_cycles
+    call (sweep, plaquette, W_temp; the pair list goes up and the step's
+    acceptance, plaquette and loops come back to the host), or with per_call
+    the three single calls sweep, plaquette, W_temp (each a host round trip)."""
     pairs = np.array(PAIRS, dtype=np.int32)
     t0 = time.perf_counter()
     for _ in range(steps):
-        g.metropolis(BETA, 0.0, NHITS, 1, proposal="exp", eps=eps)
-        g.plaquette()
-        g.wilson_loop_temporal(pairs)
+        if per_call:
+            g.metropolis(BETA, 0.0, NHITS, 1, proposal="exp", eps=eps)
+            g.plaquette()
+            g.wilson_loop_temporal(pairs)
+        else:
+            g.run_cycles(BETA, 0.0, NHITS, 1, "exp", eps, True, pairs)
     dt = time.perf_counter() - t0
-    h2d = pairs.nbytes * 3  # the pair list goes up once per spatial direction
-    d2h = 8 + 8 + 8 * len(PAIRS) * 3
+    if per_call:
+        h2d = pairs.nbytes * 3  # the pair list goes up once per spatial direction
+        d2h = 8 + 8 + 8 * len(PAIRS) * 3
+    else:
+        h2d = pairs.nbytes
+        d2h = 8 + 8 + 8 * len(PAIRS)
     return dt, h2d, d2h
 
 
@@ -278,7 +288,6 @@ def cpu_baseline_reference(L: int):
     """klft's own code (oracle/_ref shim) on the host cores: one cycle of the same workload."""
     from oracle.oracle import REF_SO, Lat, RefShim
     if not os.path.exists(REF_SO):
-        from oracle.oracle import Oracle
         return None
     r = RefShim()
     cores = r.set_threads(os.cpu_count() or 1)
@@ -288,15 +297,22 @@ def cpu_baseline_reference(L: int):
     t0 = time.perf_counter()
     r.cycles(lat, U, BETA, 0.1, NHITS, 1, 1234, PAIRS)
     dt = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    r.plaquette(lat, U)
+    dtp = time.perf_counter() - t0
     return {"value": lat.V * 4 / dt, "unit": "link updates/s", "cores": cores, "kind": "reference",
             "sample": f"1 cycle of SU(3) {L}^4 (sweep + plaquette + 64 temporal Wilson loops), klft's headers on "
                       f"the project's Kokkos-API OpenMP shim, reference SU(3) proposal, {cores} threads, "
-                      f"{dt:.2f} s"}
+                      f"{dt:.2f} s",
+            "plaquettes_per_s": lat.V * 6 / dtp,
+            "note": "klft's code and this library share the cycle's structure, but klft's SU(3) proposal is its "
+                    "Gram-Schmidt generator (an exp(i eps H) proposal does not exist there) and this cycle starts "
+                    "cold, not from the GPU arm's thermalised configuration"}
 
 
 # DRAM traffic of one link pass (dram__bytes_read.sum + dram__bytes_write.sum of one
 # metropolis_exp_kernel launch in the ncu capture summarised in the profile below).
-TRAFFIC_PASS_BYTES = 204544000 + 17146624
+TRAFFIC_PASS_BYTES = 204574976 + 18085888
 TRAFFIC_SOURCE = "profiles/metropolis_exp_su3_32x4_mixed.md"
 
 
@@ -363,21 +379,37 @@ def bench_batched_ptbc(cycles: int, warmup: int = 3):
         links += 4 * 16 ** 4
     c_of_label = [1.0 - r / 11.0 for r in range(12)]
     b.set_ptbc(list(range(12)), c_of_label, 6.0, 99)
+    su2_beta = []
     for k in range(48):
         L = [int(x) for x in rng.choice([8, 12, 16, 20, 24], size=4)]
         g = klft_b200.GaugeField(L, 2, "mixed", "hot", 7000 + k)
         g.set_stream(7000, k)
-        b.add(g, float(rng.uniform(2.2, 2.6)), 0.3, NHITS, "reference", 0.0)
+        su2_beta.append(float(rng.uniform(2.2, 2.6)))
+        b.add(g, su2_beta[-1], 0.3, NHITS, "reference", 0.0)
         fields.append(g)
         links += 4 * int(np.prod(L))
     b.run(warmup, True, True)
     acc, plaq, lab, ms = b.run(cycles, True, True)
     _, _, _, ms_ng = b.run(max(cycles // 4, 2), True, False)
     swaps = b.swap_stats()
+    # the two groups alone (their launches overlap on forked streams in the full cycle)
+    parts = {}
+    for name, sel in (("replicas_only", fields[:12]), ("su2_chains_only", fields[12:])):
+        bp = klft_b200.Batch()
+        for k, g in enumerate(sel):
+            if name == "replicas_only":
+                bp.add(g, 6.0, 0.0, NHITS, "exp", 0.25)
+            else:
+                bp.add(g, su2_beta[k], 0.3, NHITS, "reference", 0.0)
+        bp.run(2, True, True)
+        _, _, _, msp = bp.run(max(cycles // 4, 4), True, True)
+        parts[name] = msp / max(cycles // 4, 4)
+        bp.close()
     out = {"workload": "12 PTBC SU(3) 16^4 replicas (L_d=4, c_r=1-r/11, beta=6) + 48 SU(2) chains "
                        "extents {8..24}^4, beta U[2.2,2.6]; per cycle 1 sweep + swaps + plaquettes, CUDA graph",
            "chains": len(fields), "cycles": cycles, "ms_per_cycle": ms / cycles,
            "ms_per_cycle_without_graph": ms_ng / max(cycles // 4, 2),
+           "ms_per_cycle_groups_alone": parts,
            "link_updates_per_s": links * cycles / (ms * 1e-3),
            "cycles_per_s": cycles / (ms * 1e-3),
            "replica_acceptance": float(np.mean(acc[:, :12])), "su2_acceptance": float(np.mean(acc[:, 12:])),
@@ -611,9 +643,14 @@ def run_ours(a, dist: Dist):
     dist.barrier()
     e2e_dt, h2d, d2h = e2e_public_api(g, eps, e2e_steps)
     e2e_dt = dist.max(e2e_dt)
+    dist.barrier()
+    pc_dt, _, _ = e2e_public_api(g, eps, e2e_steps, per_call=True)
+    pc_dt = dist.max(pc_dt)
     e2e = {"value": links_per_step * e2e_steps * dist.world / e2e_dt, "unit": "link updates/s",
            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-           "path": "klft_metropolis_sweeps + klft_plaquette + klft_wilson_loop_temporal per step, host wall clock"}
+           "path": "klft_run_cycles per step (sweep + plaquette + W_temp, results to the host), host wall clock",
+           "value_per_call": links_per_step * e2e_steps * dist.world / pc_dt,
+           "path_per_call": "klft_metropolis_sweeps + klft_plaquette + klft_wilson_loop_temporal per step"}
     dist.barrier()
     hl_dt, hb, db = e2e_host_lattice(g, eps, 3)
     hl_dt = dist.max(hl_dt)
@@ -658,8 +695,12 @@ def run_ours(a, dist: Dist):
         "clocks": clocks.summary(), "gpu_launches": launches_per_step * a.steps,
     }
     pl_ms = plaquette_ms(g, eps)
+    pl_bytes = V * 4 * 6 * 8  # every two-row FP32 link read once
     line["plaquettes_per_s"] = {"value": V * 6 / (pl_ms * 1e-3), "ms": pl_ms,
-                                "note": "V*Nd(Nd-1)/2 plaquettes per GaugePlaquette, device time"}
+                                "hbm": {"algorithmic_bytes": pl_bytes, "achieved_gbs": pl_bytes / (pl_ms * 1e-3) / 1e9,
+                                        "frac": (pl_bytes / (pl_ms * 1e-3) / 1e9 / hbm) if hbm else None},
+                                "note": "V*Nd(Nd-1)/2 plaquettes per GaugePlaquette, device time; issue-bound "
+                                        "(profiles/plaquette_hmc_streams_batch_pass.md)"}
     if dist.world == 1 and not a.no_extras:
         for key, fn in (("c1_u1_8x4", lambda: bench_c1(not a.no_cpu_baseline)),
                         ("batched_ptbc", lambda: bench_batched_ptbc(a.batch_cycles)),
