@@ -636,7 +636,7 @@ def run_ours(a, dist: Dist):
                 "cuda_core": {"achieved_tflops": tflops, "peak_tflops": fp32, "frac": (tflops / fp32) if fp32 else None,
                               "flop_per_link_update": flop_lu,
                               "peak_source": "klft_peak_flops (measured FP32 FMA throughput)",
-                              "note": "the binding roof: ~65 flop per algorithmic byte, above the FP32 ridge"},
+                              "note": "the binding roof: ~86 flop per algorithmic byte, above the FP32 ridge of ~11"},
                 "cuda_core_peak_tflops": {"fp32": fp32, "fp64": fp64}}
     # whole-job end-to-end rates: every rank's steps over the slowest rank's wall clock
     e2e_steps = max(2, a.steps // 2)
@@ -676,6 +676,20 @@ def run_ours(a, dist: Dist):
                      "ms_sweep": s64, "ms_measure": m64, "mean_plaquette": float(np.mean(plaq64))}
         g64.close()
     mixed_err = mixed_errors(g, L)
+    # like for like with the reference arm: klft's own SU(3) proposal (delta 0.1)
+    # from a cold start, the same cycle (sweep + plaquette + 64 W_temp), FP64
+    # and mixed, on this GPU
+    same_chain = {}
+    for prec in ("fp64", "mixed"):
+        gr = klft_b200.GaugeField(L, 3, prec, "cold", 1234)
+        gr.set_stream(1234, dist.rank)
+        gr.run_cycles(BETA, 0.1, NHITS, 2, "reference", 0.0, True, PAIRS)
+        _, _, _, msr = gr.run_cycles(BETA, 0.1, NHITS, 5, "reference", 0.0, True, PAIRS)
+        msr = dist.max(msr)
+        same_chain[prec] = {"value": links_per_step * 5 * dist.world / (msr * 1e-3), "ms_per_step": msr / 5}
+        gr.close()
+    same_chain["note"] = ("klft's SU(3) Gram-Schmidt proposal (SUN.hpp:192-251) and a cold start, the chain the "
+                          "reference arm runs; link updates/s, CUDA events")
     # 8 link passes + counter advance + plaquette and its reduction + the axial-gauge
     # transform (once, shared by the spatial planes) + 3 planes x (U', loops, reduction)
     launches_per_step = npass + 1 + 2 + 1 + 3 * 3
@@ -690,7 +704,7 @@ def run_ours(a, dist: Dist):
                    "l2": f"inputs larger than L2 ({V * 4 * 6 * 8 / 1e6:.0f} MB of FP32 links, two rows stored)"},
         "breakdown_ms": {"sweep": ms_sweep, "measure": ms_meas},
         "acceptance": float(np.mean(acc)), "mean_plaquette": float(np.mean(plaq)),
-        "fp64": fp64_line, "mixed_error": mixed_err,
+        "fp64": fp64_line, "mixed_error": mixed_err, "reference_proposal": same_chain,
         "roofline": roofline, "e2e": e2e, "e2e_host_lattice": e2e_host,
         "clocks": clocks.summary(), "gpu_launches": launches_per_step * a.steps,
     }

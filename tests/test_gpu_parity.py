@@ -100,8 +100,11 @@ def test_metropolis_trajectory_matches_oracle(oracle, nd, nc, L):
     g.close()
 
 
-@pytest.mark.parametrize("L", [[4, 4, 4, 4], [6, 4, 2, 4]])
+@pytest.mark.parametrize("L", [[4, 4, 4, 4], [6, 4, 2, 4], [6, 4, 6, 4], [10, 6, 4], [8, 6], [4, 12], [12, 10, 6, 4]])
 def test_metropolis_su3_exp_proposal_matches_oracle(oracle, L):
+    """The exp(i eps H) link passes hit by hit against the oracle, in 2, 3 and 4
+    dimensions and with half-volumes that are not multiples of the 32-site
+    chunks a pass is laid out in (6, 36, 60, 12, 180 ...)."""
     lat = Lat(3, L)
     U = oracle.init(lat, True, 8)
     g = gf(L, 3)
@@ -112,6 +115,13 @@ def test_metropolis_su3_exp_proposal_matches_oracle(oracle, L):
     np.testing.assert_array_equal(acc_g, acc_o)
     np.testing.assert_allclose(g.download(), U, rtol=0, atol=1e-11)
     assert g.unitarity() < 1e-13
+    # the mixed form on the same start follows within FP32 rounding for one sweep
+    m = gf(L, 3, "mixed")
+    m.upload(oracle.init(lat, True, 8))
+    m.set_stream(2024, 0)
+    acc_m = m.metropolis(6.0, 0.0, 6, 1, proposal="exp", eps=0.35)
+    assert abs(acc_m[0] - acc_g[0]) < 0.02
+    m.close()
 
 
 def test_mixed_form_follows_fp64_chain(oracle):
