@@ -9,8 +9,9 @@
 // it is copied here in chunks through two page-locked staging buffers owned by
 // the library: host threads fill (or drain) one buffer while the DMA engine
 // moves the other, and the device-side layout conversion runs on the device
-// copy afterwards.  The staging buffers (2 x 32 MB) are allocated on first use
-// and kept for the life of the process.
+// copy afterwards.  The staging buffers (2 x 32 MB per device used) are
+// allocated on first use and kept for the life of the process; transfers on
+// one device take turns on them.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -117,12 +118,14 @@ void par_memcpy(void *dst, const void *src, size_t n) {
   });
 }
 
+// per device: the events belong to the device that created them
+constexpr int kMaxDevices = 64;
 struct Staging {
   std::mutex mu;
   void *buf[2] = {nullptr, nullptr};
   cudaEvent_t ev[2] = {nullptr, nullptr};
 };
-Staging g_staging;
+Staging g_staging[kMaxDevices];
 
 bool is_pinned(const void *p) {
   cudaPointerAttributes at;
@@ -133,38 +136,51 @@ bool is_pinned(const void *p) {
   return at.type == cudaMemoryTypeHost;
 }
 
-cudaError_t staging_ready() {
-  if (g_staging.buf[0]) return cudaSuccess;
-  for (int k = 0; k < 2; ++k) {
-    cudaError_t e = cudaHostAlloc(&g_staging.buf[k], kChunk, cudaHostAllocDefault);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g_staging.ev[k], cudaEventDisableTiming);
-    if (e != cudaSuccess) return e;
+// the current device's staging buffers (allocated on first use), or null
+Staging *staging_ready(cudaError_t &e) {
+  int dev = 0;
+  if ((e = cudaGetDevice(&dev)) != cudaSuccess) return nullptr;
+  if (dev < 0 || dev >= kMaxDevices) {
+    e = cudaErrorInvalidDevice;
+    return nullptr;
   }
-  return cudaSuccess;
+  Staging &st = g_staging[dev];
+  st.mu.lock();
+  if (!st.buf[0] || !st.buf[1] || !st.ev[0] || !st.ev[1]) {
+    for (int k = 0; k < 2; ++k) {
+      if (!st.buf[k] && (e = cudaHostAlloc(&st.buf[k], kChunk, cudaHostAllocDefault)) != cudaSuccess) break;
+      if (!st.ev[k] && (e = cudaEventCreateWithFlags(&st.ev[k], cudaEventDisableTiming)) != cudaSuccess) break;
+    }
+    if (e != cudaSuccess) {
+      st.mu.unlock();
+      return nullptr;
+    }
+  }
+  return &st;  // locked; the caller unlocks
 }
 
 }  // namespace
 
 cudaError_t copy_host_to_device(void *dst, const void *src, size_t bytes, cudaStream_t st) {
   if (is_pinned(src)) return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st);
-  std::lock_guard<std::mutex> lk(g_staging.mu);
-  cudaError_t e = staging_ready();
-  if (e != cudaSuccess) return e;
+  cudaError_t e = cudaSuccess;
+  Staging *sg = staging_ready(e);
+  if (!sg) return e;
+  std::lock_guard<std::mutex> lk(sg->mu, std::adopt_lock);
   size_t off = 0;
   for (int k = 0; off < bytes; ++k) {
     const int b = k & 1;
     const size_t n = std::min(kChunk, bytes - off);
     // the buffer's previous transfer must have left it before it is refilled
-    if ((e = cudaEventSynchronize(g_staging.ev[b])) != cudaSuccess) return e;
-    par_memcpy(g_staging.buf[b], (const char *)src + off, n);
-    if ((e = cudaMemcpyAsync((char *)dst + off, g_staging.buf[b], n, cudaMemcpyHostToDevice, st)) != cudaSuccess)
-      return e;
-    if ((e = cudaEventRecord(g_staging.ev[b], st)) != cudaSuccess) return e;
+    if ((e = cudaEventSynchronize(sg->ev[b])) != cudaSuccess) return e;
+    par_memcpy(sg->buf[b], (const char *)src + off, n);
+    if ((e = cudaMemcpyAsync((char *)dst + off, sg->buf[b], n, cudaMemcpyHostToDevice, st)) != cudaSuccess) return e;
+    if ((e = cudaEventRecord(sg->ev[b], st)) != cudaSuccess) return e;
     off += n;
   }
-  // the staging buffers are shared by all lattices: drain before returning
+  // the staging buffers are shared by all lattices of the device: drain before returning
   for (int b = 0; b < 2; ++b)
-    if ((e = cudaEventSynchronize(g_staging.ev[b])) != cudaSuccess) return e;
+    if ((e = cudaEventSynchronize(sg->ev[b])) != cudaSuccess) return e;
   return cudaSuccess;
 }
 
@@ -173,9 +189,10 @@ cudaError_t copy_device_to_host(void *dst, const void *src, size_t bytes, cudaSt
     cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st);
     return e == cudaSuccess ? cudaStreamSynchronize(st) : e;
   }
-  std::lock_guard<std::mutex> lk(g_staging.mu);
-  cudaError_t e = staging_ready();
-  if (e != cudaSuccess) return e;
+  cudaError_t e = cudaSuccess;
+  Staging *sg = staging_ready(e);
+  if (!sg) return e;
+  std::lock_guard<std::mutex> lk(sg->mu, std::adopt_lock);
   const size_t nchunks = (bytes + kChunk - 1) / kChunk;
   // chunk k goes to buffer k & 1; it is drained to the caller once its copy is
   // done, while the next chunk's copy runs
@@ -183,17 +200,16 @@ cudaError_t copy_device_to_host(void *dst, const void *src, size_t bytes, cudaSt
     if (k < nchunks) {
       const int b = (int)(k & 1);
       const size_t off = k * kChunk, n = std::min(kChunk, bytes - off);
-      if ((e = cudaMemcpyAsync(g_staging.buf[b], (const char *)src + off, n, cudaMemcpyDeviceToHost, st)) !=
-          cudaSuccess)
+      if ((e = cudaMemcpyAsync(sg->buf[b], (const char *)src + off, n, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
         return e;
-      if ((e = cudaEventRecord(g_staging.ev[b], st)) != cudaSuccess) return e;
+      if ((e = cudaEventRecord(sg->ev[b], st)) != cudaSuccess) return e;
     }
     if (k >= 1) {
       const size_t j = k - 1;
       const int b = (int)(j & 1);
       const size_t off = j * kChunk, n = std::min(kChunk, bytes - off);
-      if ((e = cudaEventSynchronize(g_staging.ev[b])) != cudaSuccess) return e;
-      par_memcpy((char *)dst + off, g_staging.buf[b], n);
+      if ((e = cudaEventSynchronize(sg->ev[b])) != cudaSuccess) return e;
+      par_memcpy((char *)dst + off, sg->buf[b], n);
     }
   }
   return cudaSuccess;
