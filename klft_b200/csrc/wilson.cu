@@ -24,7 +24,9 @@
 // Omega is stored row major (row b, column c at b*ncols + c) and U' column major
 // (c*rows + b), one plane per complex colour entry: the kernels that write them
 // run lanes over columns, the loop kernel reads U' with lanes over rows.
+#include <algorithm>
 #include <cstring>
+#include <type_traits>
 
 #include "common.cuh"
 #include "kernels.cuh"
@@ -63,31 +65,50 @@ KLFT_HD ColGeom make_colgeom(const Geom &g, int mu, int nu, int rows) {
   return c;
 }
 
-// site of (column, row) with row < L_nu
-KLFT_D Site col_site(const ColGeom &c, long long col, int row) {
+// Coordinates of a column along the dimensions other than nu (x[nu] = 0), in
+// 32-bit arithmetic whenever the column count allows it (a 64-bit division
+// by a run-time extent costs several times a 3x3 product).
+KLFT_D void col_coords(const ColGeom &c, long long col, int x[4]) {
+  if (c.ncols <= 0xffffffffLL) {
+    unsigned u = (unsigned)col;
+#pragma unroll
+    for (int d = 0; d < 4; ++d) {
+      if (d == c.nu || d >= c.nd) {
+        x[d] = 0;
+      } else {
+        const unsigned Ld = (unsigned)c.L[d], qd = u / Ld;
+        x[d] = (int)(u - qd * Ld);
+        u = qd;
+      }
+    }
+  } else {
+#pragma unroll
+    for (int d = 0; d < 4; ++d) {
+      if (d == c.nu || d >= c.nd) {
+        x[d] = 0;
+      } else {
+        x[d] = (int)(col % c.L[d]);
+        col /= c.L[d];
+      }
+    }
+  }
+}
+
+// site of the column with coordinates x at row < L_nu
+KLFT_D Site col_site_at(const ColGeom &c, const int x[4], int row) {
   Site s;
 #pragma unroll
   for (int d = 0; d < 4; ++d) {
-    int x;
-    if (d == c.nu) {
-      x = row;
-    } else if (d < c.nd) {
-      x = (int)(col % c.L[d]);
-      col /= c.L[d];
-    } else {
-      x = 0;
-    }
-    s.set_b(d, x & 1);
-    s.set_h(d, x >> 1);
+    const int v = d == c.nu ? row : x[d];
+    s.set_b(d, v & 1);
+    s.set_h(d, v >> 1);
   }
   return s;
 }
 
-// column index of xbar + k mu
-KLFT_D long long col_shift(const ColGeom &c, long long col, int k) {
-  const int Lm = c.Lmu;
-  const int xm = (int)((col / c.csmu) % Lm);
-  const int xn = (xm + k) % Lm;
+// column index of xbar + k mu, with xm the column's coordinate along mu
+KLFT_D long long col_shift_at(const ColGeom &c, long long col, int xm, int k) {
+  const int xn = (xm + k) % c.Lmu;
   return col + (long long)(xn - xm) * c.csmu;
 }
 
@@ -138,10 +159,12 @@ __global__ void omega_kernel(Links<N, T> U, Geom g, ColGeom c, CField<N, T> om, 
   const long long col = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (col >= c.ncols) return;
   const int Ln = c.Lnu;
+  int x[4];
+  col_coords(c, col, x);
   Mat<N, double> O = mident<N, double>();
   for (int b = 0; b < Ln; ++b) {
     om.store((long long)b * c.ncols + col, O);
-    O = mul(O, to_d(U.load(site_lin(g, col_site(c, col, b)), c.nu)));
+    O = mul(O, to_d(U.load(site_lin(g, col_site_at(c, x, b)), c.nu)));
   }
   pol.store(col, O);
 }
@@ -165,8 +188,11 @@ __global__ void __launch_bounds__(32 * UP_RB) uprime_kernel(Links<N, T> U, Geom 
   const int Ln = c.Lnu;
   if (col < c.ncols && row < c.rows) {
     const int b = row % Ln, k = row / Ln;
-    const long long cp = col_shift(c, col, 1);
-    const Mat<N, T> u = U.load(site_lin(g, col_site(c, col, b)), c.mu);
+    int x[4];
+    col_coords(c, col, x);
+    const int xm = c.mu == 0 ? x[0] : c.mu == 1 ? x[1] : c.mu == 2 ? x[2] : x[3];
+    const long long cp = col_shift_at(c, col, xm, 1);
+    const Mat<N, T> u = U.load(site_lin(g, col_site_at(c, x, b)), c.mu);
     Mat<N, T> v = mul_nd(mul(om.load_t((long long)b * c.ncols + col), u), om.load_t((long long)b * c.ncols + cp));
     if (k > 0) {
       const Mat<N, T> P = pol.load_t(col), Pp = pol.load_t(cp);
@@ -443,6 +469,199 @@ __global__ void __launch_bounds__(WL_THREADS, WLMinBlocks<T>::v)
   }
 }
 
+// ---------------------------------------------------------------------------
+// Column-correlation form of the loop kernel (link precision FP32, every
+// requested T in 1..WC_TW).  For a fixed column and loop length L,
+//   sum_r W_{L,T}(col, r) = sum_r sum_k v_k(r) v_k(r + T),
+// with v(r) the 2 N^2 real components of S'_L(col, r): per column it is the
+// autocorrelation at lags T = 1..8 of a sequence of 2 N^2-vectors along the nu
+// axis.  A CTA holds WC_CW columns x (32 origin + 8 halo) rows.  Per L each
+// thread first extends the lines of two rows of its column (the running
+// product S'_L = S'_{L-1} U'(x + (L-1) mu) stays in its registers) and writes
+// them to shared memory component by component; after one barrier each
+// "consumer" thread loads one component of a whole column (or of a chunk of
+// its origin rows, for N < 3) into registers and forms all eight lags there:
+// 8 x 32 FMAs per component per column from 40 shared loads, where the
+// entry-per-origin form re-reads ten 3x3 entries per two origins.
+constexpr int WC_TW = 8;        // lags T = 1..WC_TW
+constexpr int WC_RO = 32;       // origin rows per tile
+constexpr int WC_ROWS = WC_RO + WC_TW;
+constexpr int WC_PT = WC_ROWS / 2;  // threads per column: two rows each
+constexpr int WC_CW = 8;        // columns per CTA
+constexpr int WC_THREADS = WC_PT * WC_CW;  // 160: five warps
+constexpr int WC_WARPS = WC_THREADS / 32;
+constexpr int WC_RS = 44;       // floats per component row (11 x 16 B: odd, so 16-byte loads of lanes a row apart miss each other's banks)
+
+// Floats per column block: 2 N^2 component rows, padded so that consecutive
+// columns start 20 banks apart (the 20 producer lanes of a column then cover
+// distinct banks, and so do those of the next column in the same warp), and to
+// a multiple of 4 floats.
+template <int N> struct WCCol {
+  static constexpr int raw = 2 * N * N * WC_RS;
+  static constexpr int v = raw + ((20 - raw % 32 + 32) % 32);
+  static_assert(v % 4 == 0, "column blocks must stay 16-byte aligned");
+};
+// consumer work per column: component k of origin chunk c, NCH chunks of 32 / NCH rows
+template <int N> struct WCChunks { static constexpr int v = N == 3 ? 1 : N == 2 ? 2 : 8; };
+
+struct WCTable {
+  int lmax, npairs, R, ntile_rows;
+  long long ntiles;
+  short pm[WL_MAXP + 1][WC_TW];  // pair index of (L, T = j + 1), or -1
+};
+
+// Sum of v[0..7] over the warp in FP32: on return lanes with (lane & 3) == 0
+// hold the total of index (lane >> 2) & 7.
+KLFT_D float warp_transpose_sum8f(float v[8], int lane) {
+  const bool b16 = lane & 16, b8 = lane & 8, b4 = lane & 4;
+  float w[4], x[2];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const float send = b16 ? v[k] : v[k + 4];
+    const float keep = b16 ? v[k + 4] : v[k];
+    w[k] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+  }
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const float send = b8 ? w[k] : w[k + 2];
+    const float keep = b8 ? w[k + 2] : w[k];
+    x[k] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+  }
+  const float send = b4 ? x[0] : x[1];
+  float y = (b4 ? x[1] : x[0]) + __shfl_xor_sync(0xffffffffu, send, 4);
+  y += __shfl_xor_sync(0xffffffffu, y, 2);
+  y += __shfl_xor_sync(0xffffffffu, y, 1);
+  return y;
+}
+
+// a[t] += sum_{r < NV} win[r] win[r + 1 + t]; NV = n (all origins valid) at compile time
+template <int W, int NO>
+KLFT_D void wc_lags(const float (&win)[W], float (&a)[WC_TW], int nv) {
+  if (nv >= NO) {
+#pragma unroll
+    for (int r = 0; r < NO; ++r)
+#pragma unroll
+      for (int t = 0; t < WC_TW; ++t) a[t] = fmaf(win[r], win[r + 1 + t], a[t]);
+  } else {
+#pragma unroll
+    for (int r = 0; r < NO; ++r) {
+      const float o = r < nv ? win[r] : 0.f;
+#pragma unroll
+      for (int t = 0; t < WC_TW; ++t) a[t] = fmaf(o, win[r + 1 + t], a[t]);
+    }
+  }
+}
+
+template <int N>
+__global__ void __launch_bounds__(WC_THREADS, 3)
+    wcorr_kernel(CField<N, float> up, ColGeom c, const __grid_constant__ WCTable w, int tmax, double *part) {
+  constexpr int KC = 2 * N * N;
+  constexpr int NCH = WCChunks<N>::v;
+  constexpr int NO = WC_RO / NCH;  // origin rows per consumer
+  constexpr int W = NO + WC_TW;    // window
+  constexpr int CS = WCCol<N>::v;
+  static_assert(KC * NCH <= WC_PT, "consumer tasks must fit the threads of a column");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float *buf = (float *)smem_raw;                           // [2][WC_CW][CS]
+  double *acc = (double *)(buf + 2 * WC_CW * CS);          // [npairs][WC_WARPS]
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int cc = tid / WC_PT, q = tid % WC_PT;
+  for (int i = tid; i < 2 * WC_CW * CS; i += WC_THREADS) buf[i] = 0.f;  // rows never written stay finite
+  for (int p = tid; p < w.npairs * WC_WARPS; p += WC_THREADS) acc[p] = 0.0;
+  const bool consumer = q < KC * NCH;
+  const int kq = q % KC, ob = (q / KC) * NO;  // consumer's component and first origin row
+  int stage = 0;
+  __syncthreads();
+  for (long long tile = blockIdx.x; tile < w.ntiles; tile += gridDim.x) {
+    const long long ctile = tile / w.ntile_rows;
+    const int r0 = (int)(tile - ctile * w.ntile_rows) * w.R;
+    const int reff = min(w.R, c.Lnu - r0);  // origin rows of this tile
+    const int rneed = reff + tmax;           // rows read as origins or partners
+    const long long col = ctile * WC_CW + cc;
+    const bool col_ok = col < c.ncols;
+    const int xm = col_ok ? (int)((col / c.csmu) % c.Lmu) : 0;
+    long long colL = col;
+    int xl = xm;
+    Mat<N, float> S0, S1;  // S'_L at rows q and q + WC_PT of this column
+    for (int L = 1; L <= w.lmax; ++L) {
+      if (L > 1) {
+        if (++xl == c.Lmu) {
+          xl = 0;
+          colL -= (long long)(c.Lmu - 1) * c.csmu;
+        } else {
+          colL += c.csmu;
+        }
+      }
+      float *sb = buf + (stage * WC_CW + cc) * CS;
+      if (col_ok) {
+        const long long cbase = colL * c.rows + r0;
+        if (q < rneed) {
+          const Mat<N, float> u = up.load_t(cbase + q);
+          S0 = L == 1 ? u : mul(S0, u);
+#pragma unroll
+          for (int a = 0; a < N * N; ++a) {
+            sb[(2 * a) * WC_RS + q] = S0.e[a / N][a % N].re;
+            sb[(2 * a + 1) * WC_RS + q] = S0.e[a / N][a % N].im;
+          }
+        }
+        if (q + WC_PT < rneed) {
+          const Mat<N, float> u = up.load_t(cbase + q + WC_PT);
+          S1 = L == 1 ? u : mul(S1, u);
+#pragma unroll
+          for (int a = 0; a < N * N; ++a) {
+            sb[(2 * a) * WC_RS + q + WC_PT] = S1.e[a / N][a % N].re;
+            sb[(2 * a + 1) * WC_RS + q + WC_PT] = S1.e[a / N][a % N].im;
+          }
+        }
+      }
+      __syncthreads();
+      float a[WC_TW];
+#pragma unroll
+      for (int t = 0; t < WC_TW; ++t) a[t] = 0.f;
+      if (consumer && col_ok) {
+        float win[W];
+        const float4 *src = (const float4 *)(sb + kq * WC_RS + ob);
+#pragma unroll
+        for (int i = 0; i < W / 4; ++i) {
+          const float4 v = src[i];
+          win[4 * i] = v.x;
+          win[4 * i + 1] = v.y;
+          win[4 * i + 2] = v.z;
+          win[4 * i + 3] = v.w;
+        }
+        wc_lags<W, NO>(win, a, reff - ob);
+      }
+      const float tot = warp_transpose_sum8f(a, lane);
+      const int j = (lane >> 2) & 7;
+      if ((lane & 3) == 0) {
+        const int p = w.pm[L][j];
+        if (p >= 0) acc[p * WC_WARPS + warp] += (double)tot;
+      }
+      stage ^= 1;
+    }
+  }
+  __syncthreads();
+  for (int p = tid; p < w.npairs; p += WC_THREADS) {
+    double s = 0.0;
+#pragma unroll
+    for (int q2 = 0; q2 < WC_WARPS; ++q2) s += acc[p * WC_WARPS + q2];
+    part[(long long)p * gridDim.x + blockIdx.x] = s;
+  }
+}
+
+template <int N> static size_t wcorr_smem(int npairs) {
+  return (size_t)2 * WC_CW * WCCol<N>::v * sizeof(float) + (size_t)npairs * WC_WARPS * sizeof(double);
+}
+
+// Whether the column-correlation kernel serves this table: FP32 links and every
+// T in 1..WC_TW.
+static bool wcorr_eligible(int dtype, int tmax, const int *T, int nent) {
+  if (dtype == 0 || tmax > WC_TW) return false;
+  for (int k = 0; k < nent; ++k)
+    if (T[k] < 1 || T[k] > WC_TW) return false;
+  return true;
+}
+
 // Scratch needed by launch_wilson_gf (bytes).
 size_t wilson_gf_scratch(int nc, int dtype, const Geom &g, int nu, int tmax) {
   const size_t es = (dtype == 0 ? 16 : 8) * (size_t)nc * nc;
@@ -486,7 +705,7 @@ int wilson_gf_blocks(const Geom &g) {
 template <int N, typename T>
 static cudaError_t wilson_gf_t(const void *links, const Geom &g, const int *const *h_tab, int lmax, int tmax,
                                int npairs, int mu, int nu, bool omega_ready, void *scratch, double *d_part, int nblk,
-                               cudaStream_t st) {
+                               int *grid_used, cudaStream_t st) {
   auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
   const size_t es = sizeof(cx<T>) * N * N;
   const ColGeom c = make_colgeom(g, mu, nu, g.L[nu] + tmax);
@@ -501,6 +720,49 @@ static cudaError_t wilson_gf_t(const void *links, const Geom &g, const int *cons
   uprime_kernel<N, T><<<(unsigned)(nct * ((c.rows + UP_RB - 1) / UP_RB)), 32 * UP_RB, 0, st>>>(U, g, c, om, pol,
                                                                                              up);
   if (npairs > WL_MAXP || lmax > WL_MAXP || tmax > 32767) return cudaErrorInvalidValue;
+  if constexpr (std::is_same<T, float>::value) {
+    if (wcorr_eligible(1, tmax, h_tab[1], h_tab[0][lmax + 1])) {
+      WCTable w;
+      std::memset(&w, 0, sizeof w);
+      w.lmax = lmax;
+      w.npairs = npairs;
+      for (int L = 0; L <= WL_MAXP; ++L)
+        for (int j = 0; j < WC_TW; ++j) w.pm[L][j] = -1;
+      bool dup = false;
+      for (int L = 1; L <= lmax; ++L)
+        for (int k = h_tab[0][L]; k < h_tab[0][L + 1]; ++k) {
+          short &m = w.pm[L][h_tab[1][k] - 1];
+          dup = dup || m >= 0;
+          m = (short)h_tab[2][k];
+        }
+      if (!dup) {
+        w.R = g.L[nu] < WC_RO ? g.L[nu] : WC_RO;
+        w.ntile_rows = (g.L[nu] + w.R - 1) / w.R;
+        w.ntiles = ((c.ncols + WC_CW - 1) / WC_CW) * w.ntile_rows;
+        const size_t smem = wcorr_smem<N>(npairs);
+        // the attribute is per device: set it on every launch
+        cudaFuncSetAttribute(wcorr_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
+        static int per_sm[4] = {0, 0, 0, 0};
+        static int sms = 0;
+        if (!per_sm[N]) {
+          int dev = 0;
+          cudaGetDevice(&dev);
+          cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+          int nb = 0;
+          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, wcorr_kernel<N>, WC_THREADS, wcorr_smem<N>(WL_MAXP));
+          per_sm[N] = nb > 0 ? nb : 1;
+          if (sms <= 0) sms = 148;
+        }
+        const long long want = (long long)sms * per_sm[N];
+        const int grid = (int)std::min<long long>(std::min<long long>(want, nblk), w.ntiles > 0 ? w.ntiles : 1);
+        wcorr_kernel<N><<<grid, WC_THREADS, smem, st>>>(up, c, w, tmax, d_part);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        *grid_used = grid;
+        return cudaSuccess;
+      }
+    }
+  }
   WLTable w;
   std::memset(&w, 0, sizeof w);
   w.lmax = lmax;
@@ -524,6 +786,7 @@ static cudaError_t wilson_gf_t(const void *links, const Geom &g, const int *cons
                       (size_t)TileEnt<N, T>::bytes * w.CW * (2 * ((w.R + tmax + 1) / 2));
   cudaFuncSetAttribute(wloop_kernel<N, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   wloop_kernel<N, T><<<nblk, WL_THREADS, smem, st>>>(up, c, w, d_part);
+  *grid_used = nblk;
   return cudaGetLastError();
 }
 
@@ -531,8 +794,10 @@ cudaError_t launch_wilson_gf(int nc, int dtype, const void *links, const Geom &g
                              const int *const *h_tab, int lmax, int tmax, int npairs, bool omega_ready,
                              void *scratch, double *d_part, int nblk, double *d_out, cudaStream_t st) {
   cudaError_t e = cudaErrorInvalidValue;
-#define KLFT_WGF(NV, TV) \
-  e = wilson_gf_t<NV, TV>(links, g, h_tab, lmax, tmax, npairs, mu, nu, omega_ready, scratch, d_part, nblk, st)
+  int grid = nblk;  // CTAs that wrote partial sums
+#define KLFT_WGF(NV, TV)                                                                                          \
+  e = wilson_gf_t<NV, TV>(links, g, h_tab, lmax, tmax, npairs, mu, nu, omega_ready, scratch, d_part, nblk, &grid, \
+                          st)
   if (dtype == 0) {
     if (nc == 1) KLFT_WGF(1, double);
     else if (nc == 2) KLFT_WGF(2, double);
@@ -544,7 +809,7 @@ cudaError_t launch_wilson_gf(int nc, int dtype, const void *links, const Geom &g
   }
 #undef KLFT_WGF
   if (e != cudaSuccess) return e;
-  return launch_reduce_partials(d_part, nblk, npairs, d_out, st);
+  return launch_reduce_partials(d_part, grid, npairs, d_out, st);
 }
 
 }  // namespace klft
