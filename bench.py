@@ -677,6 +677,9 @@ def run_ours(a, dist: Dist):
     e2e_host = {"value": links_per_step * 3 * dist.world / hl_dt, "unit": "link updates/s",
                 "h2d_bytes_per_step": hb, "d2h_bytes_per_step": db,
                 "path": "upload links + cycle + download links per step, one reused ordinary (pageable) host array",
+                "pcie_bytes_per_step": 2 * V * 4 * 12 * 4,
+                "note": "the host array is klft's FP64 interchange layout; the library rounds / completes links on "
+                        "host threads so that only the two stored FP32 rows of each SU(3) link cross PCIe",
                 "value_pinned_host": links_per_step * 3 * dist.world / hp_dt,
                 "host_io": host_io_rates(g)}
     # FP64 form from the same thermalised configuration

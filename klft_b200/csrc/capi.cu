@@ -290,10 +290,18 @@ klft_status klft_lattice_set_counters(klft_lattice *lat, uint32_t sweep, uint32_
 klft_status klft_lattice_upload(klft_lattice *lat, const double *host) {
   if (!lat || !host) return fail(KLFT_EINVAL, "klft_lattice_upload: null pointer");
   LOCK(lat);
-  const size_t bytes = (size_t)lat->g.V * lat->g.nd * lat->nc * lat->nc * 16;
-  CK(lat->s_stage.ensure(bytes));
-  CK(copy_host_to_device(lat->s_stage.ptr, host, bytes, lat->stream));
-  CK(launch_import(lat->nc, lat->dtype(), lat->links, lat->g, (const double *)lat->s_stage.ptr, lat->stream));
+  const size_t nlinks = (size_t)lat->g.V * lat->g.nd;
+  if (lat->dtype() == 1) {
+    // mixed form: the host rounds the stored reals to FP32, a third of the bytes cross PCIe for SU(3)
+    CK(lat->s_stage.ensure(nlinks * link_planes(lat->nc, 1) * 2 * sizeof(float)));
+    CK(upload_links_f32(lat->s_stage.ptr, host, nlinks, lat->nc, lat->stream));
+    CK(launch_import_f32(lat->nc, lat->links, lat->g, (const float *)lat->s_stage.ptr, lat->stream));
+  } else {
+    const size_t bytes = nlinks * lat->nc * lat->nc * 16;
+    CK(lat->s_stage.ensure(bytes));
+    CK(copy_host_to_device(lat->s_stage.ptr, host, bytes, lat->stream));
+    CK(launch_import(lat->nc, lat->dtype(), lat->links, lat->g, (const double *)lat->s_stage.ptr, lat->stream));
+  }
   CK(launch_open_boundary(lat->nc, lat->dtype(), lat->links, lat->g, lat->stream));
   CK(cudaStreamSynchronize(lat->stream));
   return KLFT_OK;
@@ -318,10 +326,18 @@ klft_status klft_lattice_set_open_boundary(klft_lattice *lat, int mu) {
 klft_status klft_lattice_download(klft_lattice *lat, double *host) {
   if (!lat || !host) return fail(KLFT_EINVAL, "klft_lattice_download: null pointer");
   LOCK(lat);
-  const size_t bytes = (size_t)lat->g.V * lat->g.nd * lat->nc * lat->nc * 16;
-  CK(lat->s_stage.ensure(bytes));
-  CK(launch_export(lat->nc, lat->dtype(), lat->links, lat->g, (double *)lat->s_stage.ptr, lat->stream));
-  CK(copy_device_to_host(host, lat->s_stage.ptr, bytes, lat->stream));
+  const size_t nlinks = (size_t)lat->g.V * lat->g.nd;
+  if (lat->dtype() == 1) {
+    // mixed form: the stored FP32 reals cross PCIe, the host completes each link in FP64
+    CK(lat->s_stage.ensure(nlinks * link_planes(lat->nc, 1) * 2 * sizeof(float)));
+    CK(launch_export_f32(lat->nc, lat->links, lat->g, (float *)lat->s_stage.ptr, lat->stream));
+    CK(download_links_f32(host, lat->s_stage.ptr, nlinks, lat->nc, lat->stream));
+  } else {
+    const size_t bytes = nlinks * lat->nc * lat->nc * 16;
+    CK(lat->s_stage.ensure(bytes));
+    CK(launch_export(lat->nc, lat->dtype(), lat->links, lat->g, (double *)lat->s_stage.ptr, lat->stream));
+    CK(copy_device_to_host(host, lat->s_stage.ptr, bytes, lat->stream));
+  }
   return KLFT_OK;
 }
 

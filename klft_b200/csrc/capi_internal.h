@@ -38,6 +38,11 @@ void keep_pool_memory(int device);
 // and complete; device -> host: the data is in dst).
 cudaError_t copy_host_to_device(void *dst, const void *src, size_t bytes, cudaStream_t st);
 cudaError_t copy_device_to_host(void *dst, const void *src, size_t bytes, cudaStream_t st);
+// Mixed form: only the stored FP32 reals of each link cross PCIe (12 for SU(3),
+// 4 for SU(2), 2 for U(1)); the host side converts from / to klft's 2 N^2
+// doubles per link (lexicographic site, then direction) on the library's threads.
+cudaError_t upload_links_f32(void *dst, const double *src, size_t nlinks, int nc, cudaStream_t st);
+cudaError_t download_links_f32(double *dst, const void *src, size_t nlinks, int nc, cudaStream_t st);
 
 klft_status fail(klft_status code, const char *fmt, ...);
 klft_status cuda_fail(cudaError_t e, const char *what);

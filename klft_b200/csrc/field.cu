@@ -56,6 +56,39 @@ __global__ void export_kernel(Links<NC, T> U, Geom g, double *__restrict__ aos) 
     }
 }
 
+// Mixed form: the stored FP32 reals of each link in the interchange order
+// (link t = lex * Nd + mu holds F = 2 LinkPlanes reals at t * F), the first F
+// of its 2 N^2 interchange values.
+template <int NC>
+__global__ void import_f32_kernel(Links<NC, float> U, Geom g, const float *__restrict__ aos) {
+  constexpr int P = Links<NC, float>::P;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= g.V * g.nd) return;
+  const long long lex = t / g.nd;
+  const int mu = (int)(t - lex * g.nd);
+  const float *p = aos + t * (2 * P);
+  cx<float> *q = U.p + (long long)mu * P * U.V + site_lin(g, site_from_lex(g, lex));
+#pragma unroll
+  for (int k = 0; k < P; ++k) q[k * U.V] = mk<float>(p[2 * k], p[2 * k + 1]);
+}
+
+template <int NC>
+__global__ void export_f32_kernel(Links<NC, float> U, Geom g, float *__restrict__ aos) {
+  constexpr int P = Links<NC, float>::P;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= g.V * g.nd) return;
+  const long long lex = t / g.nd;
+  const int mu = (int)(t - lex * g.nd);
+  float *p = aos + t * (2 * P);
+  const cx<float> *q = U.p + (long long)mu * P * U.V + site_lin(g, site_from_lex(g, lex));
+#pragma unroll
+  for (int k = 0; k < P; ++k) {
+    const cx<float> v = q[k * U.V];
+    p[2 * k] = v.re;
+    p[2 * k + 1] = v.im;
+  }
+}
+
 // restoreSUN on every link; the mixed form reunitarises in FP64
 template <int NC, typename T>
 __global__ void reunitarize_kernel(Links<NC, T> U, Geom g) {
@@ -183,6 +216,24 @@ cudaError_t launch_init(int nc, int dtype, void *links, const Geom &g, int hot, 
 cudaError_t launch_import(int nc, int dtype, void *links, const Geom &g, const double *aos, cudaStream_t st) {
   KLFT_DISPATCH_NC_T(nc, dtype, (import_kernel<NC, T><<<nblocks(g.V * g.nd, 256), 256, 0, st>>>(
                                     Links<NC, T>{(cx<T> *)links, g.V}, g, aos)));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_import_f32(int nc, void *links, const Geom &g, const float *aos, cudaStream_t st) {
+  const unsigned nb = nblocks(g.V * g.nd, 256);
+  if (nc == 1) import_f32_kernel<1><<<nb, 256, 0, st>>>(Links<1, float>{(cx<float> *)links, g.V}, g, aos);
+  else if (nc == 2) import_f32_kernel<2><<<nb, 256, 0, st>>>(Links<2, float>{(cx<float> *)links, g.V}, g, aos);
+  else if (nc == 3) import_f32_kernel<3><<<nb, 256, 0, st>>>(Links<3, float>{(cx<float> *)links, g.V}, g, aos);
+  else return cudaErrorInvalidValue;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_export_f32(int nc, const void *links, const Geom &g, float *aos, cudaStream_t st) {
+  const unsigned nb = nblocks(g.V * g.nd, 256);
+  if (nc == 1) export_f32_kernel<1><<<nb, 256, 0, st>>>(Links<1, float>{(cx<float> *)links, g.V}, g, aos);
+  else if (nc == 2) export_f32_kernel<2><<<nb, 256, 0, st>>>(Links<2, float>{(cx<float> *)links, g.V}, g, aos);
+  else if (nc == 3) export_f32_kernel<3><<<nb, 256, 0, st>>>(Links<3, float>{(cx<float> *)links, g.V}, g, aos);
+  else return cudaErrorInvalidValue;
   return cudaGetLastError();
 }
 

@@ -16,11 +16,17 @@
 
 #include <algorithm>
 #include <condition_variable>
+#include <cstdint>
 #include <cstring>
 #include <functional>
 #include <mutex>
 #include <thread>
+#include <type_traits>
 #include <vector>
+
+#if defined(__x86_64__)
+#include <emmintrin.h>
+#endif
 
 #include "capi_internal.h"
 
@@ -159,7 +165,163 @@ Staging *staging_ready(cudaError_t &e) {
   return &st;  // locked; the caller unlocks
 }
 
+// [l0, l1) of n items split over the pool's threads, at least 4096 items each
+void par_range(size_t n, const std::function<void(size_t, size_t)> &fn) {
+  CopyPool &pool = CopyPool::get();
+  const int parts = (int)std::min<size_t>((size_t)pool.threads(), std::max<size_t>(1, n >> 12));
+  const size_t per = (n + parts - 1) / parts;
+  pool.run(parts, [&](int i) {
+    const size_t a = (size_t)i * per;
+    if (a < n) fn(a, std::min(n, a + per));
+  });
+}
+
+// Per link: F stored FP32 reals on the device, D = 2 N^2 interchange doubles.
+template <int NC> struct LinkReals {
+  static constexpr int F = NC == 3 ? 12 : (NC == 2 ? 4 : 2);
+  static constexpr int D = 2 * NC * NC;
+};
+
+// Links [l0, l1): the first F of the D doubles of each link, rounded to float
+// (round to nearest, as the device's conversion), into the page-locked staging
+// buffer with streaming stores (the DMA engine reads them next, not the CPU).
+template <int NC>
+void pack_links(float *dst, const double *src, size_t l0, size_t l1) {
+  constexpr int F = LinkReals<NC>::F, D = LinkReals<NC>::D;
+  for (size_t l = l0; l < l1; ++l) {
+    const double *a = src + l * D;
+    float *b = dst + (l - l0) * F;
+#if defined(__x86_64__)
+    if constexpr (F % 4 == 0) {
+#pragma unroll
+      for (int k = 0; k < F; k += 4) {
+        const __m128 lo = _mm_cvtpd_ps(_mm_loadu_pd(a + k)), hi = _mm_cvtpd_ps(_mm_loadu_pd(a + k + 2));
+        _mm_stream_ps(b + k, _mm_movelh_ps(lo, hi));
+      }
+    } else {
+      for (int k = 0; k < F; ++k) b[k] = (float)a[k];
+    }
+#else
+    for (int k = 0; k < F; ++k) b[k] = (float)a[k];
+#endif
+  }
+#if defined(__x86_64__)
+  _mm_sfence();
+#endif
+}
+
+// Links [l0, l1) from their stored FP32 reals to the D interchange doubles:
+// SU(3) row 2 = conj(row0 x row1) and SU(2) row 1 = (-conj(b), conj(a)), the
+// completions the device applies when it loads a link, formed here in FP64
+// (products of FP32 values are exact in FP64).  Streaming stores into a
+// 16-byte aligned destination (no read of the caller's lines before writing).
+template <int NC>
+void unpack_links(double *dst, const float *src, size_t l0, size_t l1) {
+  constexpr int F = LinkReals<NC>::F, D = LinkReals<NC>::D;
+  const bool nt = ((uintptr_t)dst & 15u) == 0;
+  for (size_t l = l0; l < l1; ++l) {
+    const float *a = src + (l - l0) * F;
+    double v[D];
+#pragma unroll
+    for (int k = 0; k < F; ++k) v[k] = (double)a[k];
+    if constexpr (NC == 3) {
+      // m2j = conj(m0k m1q - m0q m1k), (j, k, q) = (0, 1, 2), (1, 2, 0), (2, 0, 1)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        const int k = (j + 1) % 3, q = (j + 2) % 3;
+        const double ar = v[2 * k], ai = v[2 * k + 1], br = v[6 + 2 * q], bi = v[6 + 2 * q + 1];
+        const double cr = v[2 * q], ci = v[2 * q + 1], dr = v[6 + 2 * k], di = v[6 + 2 * k + 1];
+        v[12 + 2 * j] = (ar * br - ai * bi) - (cr * dr - ci * di);
+        v[12 + 2 * j + 1] = -((ar * bi + ai * br) - (cr * di + ci * dr));
+      }
+    } else if constexpr (NC == 2) {
+      v[4] = -v[2];
+      v[5] = v[3];
+      v[6] = v[0];
+      v[7] = -v[1];
+    }
+    double *b = dst + l * D;
+#if defined(__x86_64__)
+    if (nt) {
+#pragma unroll
+      for (int k = 0; k < D; k += 2) _mm_stream_pd(b + k, _mm_loadu_pd(v + k));
+      continue;
+    }
+#endif
+    std::memcpy(b, v, sizeof v);
+  }
+#if defined(__x86_64__)
+  _mm_sfence();
+#endif
+}
+
+template <typename F> void by_nc(int nc, F &&f) {
+  if (nc == 3) f(std::integral_constant<int, 3>());
+  else if (nc == 2) f(std::integral_constant<int, 2>());
+  else f(std::integral_constant<int, 1>());
+}
+
 }  // namespace
+
+cudaError_t upload_links_f32(void *dst, const double *src, size_t nlinks, int nc, cudaStream_t st) {
+  const int fr = nc == 3 ? 12 : (nc == 2 ? 4 : 2);
+  cudaError_t e = cudaSuccess;
+  Staging *sg = staging_ready(e);
+  if (!sg) return e;
+  std::lock_guard<std::mutex> lk(sg->mu, std::adopt_lock);
+  const size_t per_chunk = kChunk / (fr * sizeof(float));
+  for (size_t k = 0, l0 = 0; l0 < nlinks; ++k, l0 += per_chunk) {
+    const int b = (int)(k & 1);
+    const size_t n = std::min(per_chunk, nlinks - l0);
+    if ((e = cudaEventSynchronize(sg->ev[b])) != cudaSuccess) return e;
+    float *stage = (float *)sg->buf[b];
+    by_nc(nc, [&](auto ncv) {
+      constexpr int NC = decltype(ncv)::value;
+      par_range(n, [&](size_t a, size_t z) { pack_links<NC>(stage + a * fr, src, l0 + a, l0 + z); });
+    });
+    if ((e = cudaMemcpyAsync((float *)dst + l0 * fr, stage, n * fr * sizeof(float), cudaMemcpyHostToDevice, st)) !=
+        cudaSuccess)
+      return e;
+    if ((e = cudaEventRecord(sg->ev[b], st)) != cudaSuccess) return e;
+  }
+  for (int b = 0; b < 2; ++b)
+    if ((e = cudaEventSynchronize(sg->ev[b])) != cudaSuccess) return e;
+  return cudaSuccess;
+}
+
+cudaError_t download_links_f32(double *dst, const void *src, size_t nlinks, int nc, cudaStream_t st) {
+  const int fr = nc == 3 ? 12 : (nc == 2 ? 4 : 2);
+  cudaError_t e = cudaSuccess;
+  Staging *sg = staging_ready(e);
+  if (!sg) return e;
+  std::lock_guard<std::mutex> lk(sg->mu, std::adopt_lock);
+  const size_t per_chunk = kChunk / (fr * sizeof(float));
+  const size_t nchunks = (nlinks + per_chunk - 1) / per_chunk;
+  // chunk k goes to buffer k & 1 and is expanded into the caller's array once
+  // its copy is done, while the next chunk's copy runs
+  for (size_t k = 0; k < nchunks + 1; ++k) {
+    if (k < nchunks) {
+      const int b = (int)(k & 1);
+      const size_t l0 = k * per_chunk, n = std::min(per_chunk, nlinks - l0);
+      if ((e = cudaMemcpyAsync(sg->buf[b], (const float *)src + l0 * fr, n * fr * sizeof(float),
+                               cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+        return e;
+      if ((e = cudaEventRecord(sg->ev[b], st)) != cudaSuccess) return e;
+    }
+    if (k >= 1) {
+      const size_t j = k - 1;
+      const int b = (int)(j & 1);
+      const size_t l0 = j * per_chunk, n = std::min(per_chunk, nlinks - l0);
+      if ((e = cudaEventSynchronize(sg->ev[b])) != cudaSuccess) return e;
+      const float *stage = (const float *)sg->buf[b];
+      by_nc(nc, [&](auto ncv) {
+        constexpr int NC = decltype(ncv)::value;
+        par_range(n, [&](size_t a, size_t z) { unpack_links<NC>(dst, stage + a * fr, l0 + a, l0 + z); });
+      });
+    }
+  }
+  return cudaSuccess;
+}
 
 cudaError_t copy_host_to_device(void *dst, const void *src, size_t bytes, cudaStream_t st) {
   if (is_pinned(src)) return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st);

@@ -28,6 +28,9 @@ cudaError_t launch_init(int nc, int dtype, void *links, const Geom &g, int hot, 
 // host AoS FP64 staging buffer <-> device layout
 cudaError_t launch_import(int nc, int dtype, void *links, const Geom &g, const double *aos, cudaStream_t st);
 cudaError_t launch_export(int nc, int dtype, const void *links, const Geom &g, double *aos, cudaStream_t st);
+// mixed form: the stored FP32 reals per link in interchange order (see field.cu)
+cudaError_t launch_import_f32(int nc, void *links, const Geom &g, const float *aos, cudaStream_t st);
+cudaError_t launch_export_f32(int nc, const void *links, const Geom &g, float *aos, cudaStream_t st);
 // zero the links across the open boundary (no-op when periodic)
 cudaError_t launch_open_boundary(int nc, int dtype, void *links, const Geom &g, cudaStream_t st);
 cudaError_t launch_reunitarize(int nc, int dtype, void *links, const Geom &g, cudaStream_t st);

@@ -593,20 +593,20 @@ __global__ void __launch_bounds__(WC_THREADS, 3)
         }
       }
       float *sb = buf + (stage * WC_CW + cc) * CS;
-      if (col_ok) {
-        const long long cbase = colL * c.rows + r0;
-        if (q < rneed) {
-          const Mat<N, float> u = up.load_t(cbase + q);
-          S0 = L == 1 ? u : mul(S0, u);
+      if (col_ok && q < rneed) {
+        // both rows' loads in flight before the first product
+        const long long cbase = colL * c.rows + r0 + q;
+        const bool two = q + WC_PT < rneed;
+        const Mat<N, float> u0 = up.load_t(cbase);
+        const Mat<N, float> u1 = two ? up.load_t(cbase + WC_PT) : mzero<N, float>();
+        S0 = L == 1 ? u0 : mul(S0, u0);
 #pragma unroll
-          for (int a = 0; a < N * N; ++a) {
-            sb[(2 * a) * WC_RS + q] = S0.e[a / N][a % N].re;
-            sb[(2 * a + 1) * WC_RS + q] = S0.e[a / N][a % N].im;
-          }
+        for (int a = 0; a < N * N; ++a) {
+          sb[(2 * a) * WC_RS + q] = S0.e[a / N][a % N].re;
+          sb[(2 * a + 1) * WC_RS + q] = S0.e[a / N][a % N].im;
         }
-        if (q + WC_PT < rneed) {
-          const Mat<N, float> u = up.load_t(cbase + q + WC_PT);
-          S1 = L == 1 ? u : mul(S1, u);
+        if (two) {
+          S1 = L == 1 ? u1 : mul(S1, u1);
 #pragma unroll
           for (int a = 0; a < N * N; ++a) {
             sb[(2 * a) * WC_RS + q + WC_PT] = S1.e[a / N][a % N].re;
