@@ -44,23 +44,29 @@ def test_integrate_matches_oracle(oracle, nc, L, integ):
     g.set_momenta(P)
     g.hmc_integrate(2.0, 0.6, 6, integ)
     oracle.integrate(lat, U, P, 2.0, 0.6, 6, INTEG[integ])
-    np.testing.assert_allclose(g.download(), U, rtol=0, atol=1e-11)
-    np.testing.assert_allclose(g.momenta(), P, rtol=0, atol=1e-10)
+    np.testing.assert_allclose(g.download(), U, rtol=0, atol=1e-12)
+    np.testing.assert_allclose(g.momenta(), P, rtol=0, atol=1e-11)
 
 
-@pytest.mark.parametrize("nc,L", COMBOS[:3])
-def test_trajectories_match_oracle(oracle, nc, L):
+# dH = H_new - H_old is a difference of lattice sums of size ~V: its rounding
+# floor is ~1e-16 of H, not of dH, hence the absolute term for small dH.
+DH_RTOL, DH_ATOL, LINK_ATOL = 1e-12, 1e-12, 1e-12
+
+
+@pytest.mark.parametrize("nc,L", COMBOS[:3] + [(2, [8, 8, 8, 8]), (3, [8, 8, 8, 8])])
+@pytest.mark.parametrize("integ", ["leapfrog", "omelyan"])
+def test_trajectories_match_oracle(oracle, nc, L, integ):
     lat = Lat(nc, L)
     U = oracle.init(lat, True, 51)
     g = gf(L, nc)
     g.upload(U)
     g.set_stream(1001, 7)
     beta = {1: 1.0, 2: 2.3, 3: 5.5}[nc]
-    dH_g, acc_g = g.hmc(beta, 1.0, 8, 4, "leapfrog")
-    dH_o, acc_o = oracle.hmc(lat, U, beta, 1.0, 8, INTEGRATOR_LEAPFROG, 1001, 7, 0, 4)
+    dH_g, acc_g = g.hmc(beta, 1.0, 8, 4, integ)
+    dH_o, acc_o = oracle.hmc(lat, U, beta, 1.0, 8, INTEG[integ], 1001, 7, 0, 4)
     np.testing.assert_array_equal(acc_g, acc_o)
-    np.testing.assert_allclose(dH_g, dH_o, rtol=1e-8, atol=1e-9)
-    np.testing.assert_allclose(g.download(), U, rtol=0, atol=1e-10)
+    np.testing.assert_allclose(dH_g, dH_o, rtol=DH_RTOL, atol=DH_ATOL)
+    np.testing.assert_allclose(g.download(), U, rtol=0, atol=LINK_ATOL)
     assert g.counters()[1] == 4
 
 
