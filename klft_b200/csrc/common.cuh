@@ -334,8 +334,22 @@ KLFT_HD Site site_shift(const Geom &g, Site s, int d, int k) {
   s.set_h(d, x >> 1);
   return s;
 }
+// Site decodes: 32-bit arithmetic whenever the volume allows (a 64-bit
+// division by a run-time extent costs tens of instructions).
 KLFT_HD Site site_from_lin(const Geom &g, long long lin) {
   Site s;
+  if (g.V < (1LL << 31)) {
+    const unsigned vh = (unsigned)g.Vh, sub = (unsigned)lin / vh;
+    unsigned hidx = (unsigned)lin - sub * vh;
+#pragma unroll
+    for (int d = 0; d < 4; ++d) {
+      const unsigned hd = (unsigned)g.H[d], q = hidx / hd;
+      s.set_b(d, (int)((sub >> d) & 1u));
+      s.set_h(d, (int)(hidx - q * hd));
+      hidx = q;
+    }
+    return s;
+  }
   const int sub = (int)(lin / g.Vh);
   long long hidx = lin - (long long)sub * g.Vh;
 #pragma unroll
@@ -348,6 +362,18 @@ KLFT_HD Site site_from_lin(const Geom &g, long long lin) {
 }
 KLFT_HD Site site_from_lex(const Geom &g, long long lex) {
   Site s;
+  if (g.V < (1LL << 31)) {
+    unsigned r = (unsigned)lex;
+#pragma unroll
+    for (int d = 0; d < 4; ++d) {
+      const unsigned ld = (unsigned)g.L[d], q = r / ld;
+      const int x = (int)(r - q * ld);
+      r = q;
+      s.set_b(d, x & 1);
+      s.set_h(d, x >> 1);
+    }
+    return s;
+  }
 #pragma unroll
   for (int d = 0; d < 4; ++d) {
     const int x = (int)(lex % g.L[d]);

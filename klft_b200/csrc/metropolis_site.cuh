@@ -165,11 +165,10 @@ KLFT_HD long long link_pass_threads(const Geom &g, int nd) {
   return (g.Vh + 31) / 32 * 32 * (1ll << (nd - 1));
 }
 KLFT_D Site link_pass_site(const Geom &g, long long t, int p, int nd, bool &ok) {
-  const unsigned ncls = 1u << (nd - 1);
   const unsigned lane = (unsigned)(t & 31);
   const unsigned long long w = (unsigned long long)(t >> 5);
-  const unsigned c = (unsigned)(w % ncls);
-  unsigned hidx = (unsigned)((w / ncls) * 32u + lane);
+  const unsigned c = (unsigned)(w & ((1u << (nd - 1)) - 1u));  // 2^(Nd-1) classes per parity
+  unsigned hidx = (unsigned)((w >> (nd - 1)) * 32u + lane);
   ok = hidx < (unsigned)g.Vh;
   const unsigned sub = (c << 1) | ((unsigned)(__popc(c) & 1) ^ (unsigned)p);
   Site x;

@@ -26,17 +26,30 @@ KLFT_D double block_sum(double v) {
 // needs were just brought into L2 by its sibling warps.  Coalescing is kept
 // (a warp reads 32 consecutive entries of one class).
 KLFT_D bool window_site(const Geom &g, long long t, Site &x, long long &lin) {
-  const int nsub = 1 << g.nd;
+  // 2^Nd classes: shifts and masks; the half-coordinates in 32-bit arithmetic
+  // whenever the half-volume allows (a 64-bit division by a run-time extent
+  // costs tens of instructions)
   const long long w = t >> 5;
-  const int sub = (int)(w % nsub);
-  const long long hidx = (w / nsub) * 32 + (t & 31);
+  const int sub = (int)(w & ((1 << g.nd) - 1));
+  const long long hidx = (w >> g.nd) * 32 + (t & 31);
   if (hidx >= g.Vh) return false;
-  long long r = hidx;
+  if (g.Vh < (1LL << 31)) {
+    unsigned r = (unsigned)hidx;
 #pragma unroll
-  for (int d = 0; d < 4; ++d) {
-    x.set_b(d, (sub >> d) & 1);
-    x.set_h(d, (int)(r % g.H[d]));
-    r /= g.H[d];
+    for (int d = 0; d < 4; ++d) {
+      const unsigned hd = (unsigned)g.H[d], q = r / hd;
+      x.set_b(d, (sub >> d) & 1);
+      x.set_h(d, (int)(r - q * hd));
+      r = q;
+    }
+  } else {
+    long long r = hidx;
+#pragma unroll
+    for (int d = 0; d < 4; ++d) {
+      x.set_b(d, (sub >> d) & 1);
+      x.set_h(d, (int)(r % g.H[d]));
+      r /= g.H[d];
+    }
   }
   lin = (long long)sub * g.Vh + hidx;
   return true;

@@ -112,33 +112,72 @@ KLFT_D long long col_shift_at(const ColGeom &c, long long col, int xm, int k) {
   return col + (long long)(xn - xm) * c.csmu;
 }
 
+// Scratch field of N x N complex entries per site.  FP64: one plane per entry
+// (entry a of site i at a * n + i, 16 bytes).  FP32: entries in pairs, so that
+// a thread moves 16 bytes per access: entries 2q and 2q + 1 of site i share the
+// 16-byte slot q * n + i (CPairs<N> pair planes; an odd last entry has its slot
+// to itself).
+template <int N> struct CPairs { static constexpr int v = (N * N + 1) / 2; };
 template <int N, typename T> struct CField {
   cx<T> *p;
-  long long n;  // entries per colour plane
+  long long n;  // sites per plane
+  static constexpr bool paired = sizeof(T) == 4;
+  KLFT_D cx<T> get(int a, long long i) const {
+    if constexpr (paired) return p[((long long)(a >> 1) * n + i) * 2 + (a & 1)];
+    else return p[(long long)a * n + i];
+  }
+  KLFT_D Mat<N, T> load_t(long long i) const {
+    Mat<N, T> m;
+    if constexpr (paired) {
+#pragma unroll
+      for (int q = 0; q < CPairs<N>::v; ++q) {
+        const float4 v = ((const float4 *)p)[(long long)q * n + i];
+        m.e[(2 * q) / N][(2 * q) % N] = mk<T>(v.x, v.y);
+        if (2 * q + 1 < N * N) m.e[(2 * q + 1) / N][(2 * q + 1) % N] = mk<T>(v.z, v.w);
+      }
+    } else {
+#pragma unroll
+      for (int a = 0; a < N; ++a)
+#pragma unroll
+        for (int b = 0; b < N; ++b) m.e[a][b] = p[(a * N + b) * n + i];
+    }
+    return m;
+  }
   KLFT_D Mat<N, double> load(long long i) const {
+    const Mat<N, T> t = load_t(i);
     Mat<N, double> m;
 #pragma unroll
     for (int a = 0; a < N; ++a)
 #pragma unroll
-      for (int b = 0; b < N; ++b) {
-        const cx<T> v = p[(a * N + b) * n + i];
-        m.e[a][b] = mk<double>((double)v.re, (double)v.im);
-      }
+      for (int b = 0; b < N; ++b) m.e[a][b] = mk<double>((double)t.e[a][b].re, (double)t.e[a][b].im);
     return m;
   }
-  KLFT_D Mat<N, T> load_t(long long i) const {
-    Mat<N, T> m;
+  KLFT_D void store_t(long long i, const Mat<N, T> &m) const {
+    if constexpr (paired) {
 #pragma unroll
-    for (int a = 0; a < N; ++a)
+      for (int q = 0; q < CPairs<N>::v; ++q) {
+        const cx<T> x = m.e[(2 * q) / N][(2 * q) % N];
+        const cx<T> y = 2 * q + 1 < N * N ? m.e[(2 * q + 1) / N][(2 * q + 1) % N] : mk<T>(T(0), T(0));
+        ((float4 *)p)[(long long)q * n + i] = make_float4(x.re, x.im, y.re, y.im);
+      }
+    } else {
 #pragma unroll
-      for (int b = 0; b < N; ++b) m.e[a][b] = p[(a * N + b) * n + i];
-    return m;
+      for (int a = 0; a < N; ++a)
+#pragma unroll
+        for (int b = 0; b < N; ++b) p[(a * N + b) * n + i] = m.e[a][b];
+    }
   }
   KLFT_D void store(long long i, const Mat<N, double> &m) const {
+    Mat<N, T> t;
 #pragma unroll
     for (int a = 0; a < N; ++a)
 #pragma unroll
-      for (int b = 0; b < N; ++b) p[(a * N + b) * n + i] = mk<T>((T)m.e[a][b].re, (T)m.e[a][b].im);
+      for (int b = 0; b < N; ++b) t.e[a][b] = mk<T>((T)m.e[a][b].re, (T)m.e[a][b].im);
+    store_t(i, t);
+  }
+  // bytes of one field of nsites sites
+  static KLFT_HD size_t bytes(long long nsites) {
+    return (size_t)nsites * (paired ? 2 * CPairs<N>::v : N * N) * sizeof(cx<T>);
   }
 };
 
@@ -206,8 +245,10 @@ __global__ void __launch_bounds__(32 * UP_RB) uprime_kernel(Links<N, T> U, Geom 
   const long long col2 = ctile * 32 + cl2;
   const int row2 = row0 + r2;
   if (col2 < c.ncols && row2 < c.rows) {
+    Mat<N, T> m;
 #pragma unroll
-    for (int a = 0; a < N * N; ++a) up.p[(long long)a * up.n + col2 * c.rows + row2] = tile[a][r2][cl2];
+    for (int a = 0; a < N * N; ++a) m.e[a / N][a % N] = tile[a][r2][cl2];
+    up.store_t(col2 * c.rows + row2, m);
   }
 }
 
@@ -490,16 +531,21 @@ constexpr int WC_PT = WC_ROWS / 2;  // threads per column: two rows each
 constexpr int WC_CW = 8;        // columns per CTA
 constexpr int WC_THREADS = WC_PT * WC_CW;  // 160: five warps
 constexpr int WC_WARPS = WC_THREADS / 32;
-constexpr int WC_RS = 44;       // floats per component row (11 x 16 B: odd, so 16-byte loads of lanes a row apart miss each other's banks)
+// Reals per component row: 44 floats (11 x 16 B) or 42 doubles (21 x 16 B),
+// an odd number of 16-byte units, so that 16-byte loads of lanes a row apart
+// miss each other's banks.
+template <typename T> struct WCRow { static constexpr int v = 44; };
+template <> struct WCRow<double> { static constexpr int v = 42; };
+// CTAs per SM: the FP64 form holds twice the registers and shared memory
+template <typename T> struct WCMinBlocks { static constexpr int v = 3; };
+template <> struct WCMinBlocks<double> { static constexpr int v = 2; };
 
-// Floats per column block: 2 N^2 component rows, padded so that consecutive
-// columns start 20 banks apart (the 20 producer lanes of a column then cover
-// distinct banks, and so do those of the next column in the same warp), and to
-// a multiple of 4 floats.
-template <int N> struct WCCol {
-  static constexpr int raw = 2 * N * N * WC_RS;
-  static constexpr int v = raw + ((20 - raw % 32 + 32) % 32);
-  static_assert(v % 4 == 0, "column blocks must stay 16-byte aligned");
+// Reals per column block: 2 N^2 component rows, padded (FP32) so that
+// consecutive columns start 20 banks apart, and to a multiple of 16 bytes.
+template <int N, typename T> struct WCCol {
+  static constexpr int raw = 2 * N * N * WCRow<T>::v;
+  static constexpr int v = sizeof(T) == 4 ? raw + ((20 - raw % 32 + 32) % 32) : raw + (raw & 1);
+  static_assert((v * sizeof(T)) % 16 == 0, "column blocks must stay 16-byte aligned");
 };
 // consumer work per column: component k of origin chunk c, NCH chunks of 32 / NCH rows
 template <int N> struct WCChunks { static constexpr int v = N == 3 ? 1 : N == 2 ? 2 : 8; };
@@ -510,59 +556,80 @@ struct WCTable {
   short pm[WL_MAXP + 1][WC_TW];  // pair index of (L, T = j + 1), or -1
 };
 
-// Sum of v[0..7] over the warp in FP32: on return lanes with (lane & 3) == 0
-// hold the total of index (lane >> 2) & 7.
-KLFT_D float warp_transpose_sum8f(float v[8], int lane) {
+// Sum of v[0..7] over the warp in the lag precision: on return lanes with
+// (lane & 3) == 0 hold the total of index (lane >> 2) & 7.
+template <typename T> KLFT_D T warp_transpose_sum8t(T v[8], int lane) {
   const bool b16 = lane & 16, b8 = lane & 8, b4 = lane & 4;
-  float w[4], x[2];
+  T w[4], x[2];
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
-    const float send = b16 ? v[k] : v[k + 4];
-    const float keep = b16 ? v[k + 4] : v[k];
+    const T send = b16 ? v[k] : v[k + 4];
+    const T keep = b16 ? v[k + 4] : v[k];
     w[k] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
   }
 #pragma unroll
   for (int k = 0; k < 2; ++k) {
-    const float send = b8 ? w[k] : w[k + 2];
-    const float keep = b8 ? w[k + 2] : w[k];
+    const T send = b8 ? w[k] : w[k + 2];
+    const T keep = b8 ? w[k + 2] : w[k];
     x[k] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
   }
-  const float send = b4 ? x[0] : x[1];
-  float y = (b4 ? x[1] : x[0]) + __shfl_xor_sync(0xffffffffu, send, 4);
+  const T send = b4 ? x[0] : x[1];
+  T y = (b4 ? x[1] : x[0]) + __shfl_xor_sync(0xffffffffu, send, 4);
   y += __shfl_xor_sync(0xffffffffu, y, 2);
   y += __shfl_xor_sync(0xffffffffu, y, 1);
   return y;
 }
 
-// a[t] += sum_{r < NV} win[r] win[r + 1 + t]; NV = n (all origins valid) at compile time
-template <int W, int NO>
-KLFT_D void wc_lags(const float (&win)[W], float (&a)[WC_TW], int nv) {
+// a[t] += sum_{r < nv} win[r] win[r + 1 + t]; all NO origins valid when nv >= NO
+template <typename T, int W, int NO>
+KLFT_D void wc_lags(const T (&win)[W], T (&a)[WC_TW], int nv) {
   if (nv >= NO) {
 #pragma unroll
     for (int r = 0; r < NO; ++r)
 #pragma unroll
-      for (int t = 0; t < WC_TW; ++t) a[t] = fmaf(win[r], win[r + 1 + t], a[t]);
+      for (int t = 0; t < WC_TW; ++t) a[t] = fma(win[r], win[r + 1 + t], a[t]);
   } else {
 #pragma unroll
     for (int r = 0; r < NO; ++r) {
-      const float o = r < nv ? win[r] : 0.f;
+      const T o = r < nv ? win[r] : T(0);
 #pragma unroll
-      for (int t = 0; t < WC_TW; ++t) a[t] = fmaf(o, win[r + 1 + t], a[t]);
+      for (int t = 0; t < WC_TW; ++t) a[t] = fma(o, win[r + 1 + t], a[t]);
     }
   }
 }
 
-template <int N>
-__global__ void __launch_bounds__(WC_THREADS, 3)
-    wcorr_kernel(CField<N, float> up, ColGeom c, const __grid_constant__ WCTable w, int tmax, double *part) {
+// W reals of a component row into registers by 16-byte loads
+template <int W> KLFT_D void wc_window(const float *src, float (&win)[W]) {
+#pragma unroll
+  for (int i = 0; i < W / 4; ++i) {
+    const float4 v = ((const float4 *)src)[i];
+    win[4 * i] = v.x;
+    win[4 * i + 1] = v.y;
+    win[4 * i + 2] = v.z;
+    win[4 * i + 3] = v.w;
+  }
+}
+template <int W> KLFT_D void wc_window(const double *src, double (&win)[W]) {
+#pragma unroll
+  for (int i = 0; i < W / 2; ++i) {
+    const double2 v = ((const double2 *)src)[i];
+    win[2 * i] = v.x;
+    win[2 * i + 1] = v.y;
+  }
+}
+
+template <int N, typename T>
+__global__ void __launch_bounds__(WC_THREADS, WCMinBlocks<T>::v)
+    wcorr_kernel(CField<N, T> up, ColGeom c, const __grid_constant__ WCTable w, int tmax, double *part) {
   constexpr int KC = 2 * N * N;
   constexpr int NCH = WCChunks<N>::v;
   constexpr int NO = WC_RO / NCH;  // origin rows per consumer
   constexpr int W = NO + WC_TW;    // window
-  constexpr int CS = WCCol<N>::v;
+  constexpr int CS = WCCol<N, T>::v;
+  constexpr int RS = WCRow<T>::v;
   static_assert(KC * NCH <= WC_PT, "consumer tasks must fit the threads of a column");
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  float *buf = (float *)smem_raw;                           // [2][WC_CW][CS]
+  T *buf = (T *)smem_raw;                                   // [2][WC_CW][CS]
   double *acc = (double *)(buf + 2 * WC_CW * CS);          // [npairs][WC_WARPS]
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int cc = tid / WC_PT, q = tid % WC_PT;
@@ -582,7 +649,7 @@ __global__ void __launch_bounds__(WC_THREADS, 3)
     const int xm = col_ok ? (int)((col / c.csmu) % c.Lmu) : 0;
     long long colL = col;
     int xl = xm;
-    Mat<N, float> S0, S1;  // S'_L at rows q and q + WC_PT of this column
+    Mat<N, T> S0, S1;  // S'_L at rows q and q + WC_PT of this column
     for (int L = 1; L <= w.lmax; ++L) {
       if (L > 1) {
         if (++xl == c.Lmu) {
@@ -592,46 +659,51 @@ __global__ void __launch_bounds__(WC_THREADS, 3)
           colL += c.csmu;
         }
       }
-      float *sb = buf + (stage * WC_CW + cc) * CS;
+      T *sb = buf + (stage * WC_CW + cc) * CS;
       if (col_ok && q < rneed) {
         // both rows' loads in flight before the first product
         const long long cbase = colL * c.rows + r0 + q;
         const bool two = q + WC_PT < rneed;
-        const Mat<N, float> u0 = up.load_t(cbase);
-        const Mat<N, float> u1 = two ? up.load_t(cbase + WC_PT) : mzero<N, float>();
+        const Mat<N, T> u0 = up.load_t(cbase);
+        // FP32: the second row's load too (FP64 has no registers to spare for it)
+        Mat<N, T> u1;
+        if constexpr (sizeof(T) == 4) u1 = two ? up.load_t(cbase + WC_PT) : mzero<N, T>();
         S0 = L == 1 ? u0 : mul(S0, u0);
 #pragma unroll
         for (int a = 0; a < N * N; ++a) {
-          sb[(2 * a) * WC_RS + q] = S0.e[a / N][a % N].re;
-          sb[(2 * a + 1) * WC_RS + q] = S0.e[a / N][a % N].im;
+          sb[(2 * a) * RS + q] = S0.e[a / N][a % N].re;
+          sb[(2 * a + 1) * RS + q] = S0.e[a / N][a % N].im;
         }
         if (two) {
+          if constexpr (sizeof(T) == 8) u1 = up.load_t(cbase + WC_PT);
           S1 = L == 1 ? u1 : mul(S1, u1);
 #pragma unroll
           for (int a = 0; a < N * N; ++a) {
-            sb[(2 * a) * WC_RS + q + WC_PT] = S1.e[a / N][a % N].re;
-            sb[(2 * a + 1) * WC_RS + q + WC_PT] = S1.e[a / N][a % N].im;
+            sb[(2 * a) * RS + q + WC_PT] = S1.e[a / N][a % N].re;
+            sb[(2 * a + 1) * RS + q + WC_PT] = S1.e[a / N][a % N].im;
           }
         }
       }
       __syncthreads();
-      float a[WC_TW];
+      T a[WC_TW];
 #pragma unroll
-      for (int t = 0; t < WC_TW; ++t) a[t] = 0.f;
+      for (int t = 0; t < WC_TW; ++t) a[t] = T(0);
       if (consumer && col_ok) {
-        float win[W];
-        const float4 *src = (const float4 *)(sb + kq * WC_RS + ob);
-#pragma unroll
-        for (int i = 0; i < W / 4; ++i) {
-          const float4 v = src[i];
-          win[4 * i] = v.x;
-          win[4 * i + 1] = v.y;
-          win[4 * i + 2] = v.z;
-          win[4 * i + 3] = v.w;
+        if constexpr (sizeof(T) == 8 && NO % 2 == 0) {
+          // FP64: the window in two halves of the origins (the overlap reloaded)
+#pragma unroll 1
+          for (int h = 0; h < 2; ++h) {
+            T win[NO / 2 + WC_TW];
+            wc_window<NO / 2 + WC_TW>(sb + kq * RS + ob + h * (NO / 2), win);
+            wc_lags<T, NO / 2 + WC_TW, NO / 2>(win, a, reff - ob - h * (NO / 2));
+          }
+        } else {
+          T win[W];
+          wc_window<W>(sb + kq * RS + ob, win);
+          wc_lags<T, W, NO>(win, a, reff - ob);
         }
-        wc_lags<W, NO>(win, a, reff - ob);
       }
-      const float tot = warp_transpose_sum8f(a, lane);
+      const T tot = warp_transpose_sum8t<T>(a, lane);
       const int j = (lane >> 2) & 7;
       if ((lane & 3) == 0) {
         const int p = w.pm[L][j];
@@ -649,14 +721,13 @@ __global__ void __launch_bounds__(WC_THREADS, 3)
   }
 }
 
-template <int N> static size_t wcorr_smem(int npairs) {
-  return (size_t)2 * WC_CW * WCCol<N>::v * sizeof(float) + (size_t)npairs * WC_WARPS * sizeof(double);
+template <int N, typename T> static size_t wcorr_smem(int npairs) {
+  return (size_t)2 * WC_CW * WCCol<N, T>::v * sizeof(T) + (size_t)npairs * WC_WARPS * sizeof(double);
 }
 
-// Whether the column-correlation kernel serves this table: FP32 links and every
-// T in 1..WC_TW.
-static bool wcorr_eligible(int dtype, int tmax, const int *T, int nent) {
-  if (dtype == 0 || tmax > WC_TW) return false;
+// Whether the column-correlation kernel serves this table: every T in 1..WC_TW.
+static bool wcorr_eligible(int tmax, const int *T, int nent) {
+  if (tmax > WC_TW) return false;
   for (int k = 0; k < nent; ++k)
     if (T[k] < 1 || T[k] > WC_TW) return false;
   return true;
@@ -664,7 +735,8 @@ static bool wcorr_eligible(int dtype, int tmax, const int *T, int nent) {
 
 // Scratch needed by launch_wilson_gf (bytes).
 size_t wilson_gf_scratch(int nc, int dtype, const Geom &g, int nu, int tmax) {
-  const size_t es = (dtype == 0 ? 16 : 8) * (size_t)nc * nc;
+  // bytes per site of a scratch field (CField: FP32 entries in 16-byte pairs)
+  const size_t es = dtype == 0 ? 16 * (size_t)nc * nc : 16 * (size_t)((nc * nc + 1) / 2);
   const size_t rows = (size_t)g.L[nu] + (size_t)tmax;
   const size_t ncols = (size_t)(g.V / g.L[nu]);
   auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
@@ -707,7 +779,7 @@ static cudaError_t wilson_gf_t(const void *links, const Geom &g, const int *cons
                                int npairs, int mu, int nu, bool omega_ready, void *scratch, double *d_part, int nblk,
                                int *grid_used, cudaStream_t st) {
   auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
-  const size_t es = sizeof(cx<T>) * N * N;
+  const size_t es = CField<N, T>::bytes(1);
   const ColGeom c = make_colgeom(g, mu, nu, g.L[nu] + tmax);
   const long long Vc = c.ncols * g.L[nu];
   char *base = (char *)scratch;
@@ -720,8 +792,8 @@ static cudaError_t wilson_gf_t(const void *links, const Geom &g, const int *cons
   uprime_kernel<N, T><<<(unsigned)(nct * ((c.rows + UP_RB - 1) / UP_RB)), 32 * UP_RB, 0, st>>>(U, g, c, om, pol,
                                                                                              up);
   if (npairs > WL_MAXP || lmax > WL_MAXP || tmax > 32767) return cudaErrorInvalidValue;
-  if constexpr (std::is_same<T, float>::value) {
-    if (wcorr_eligible(1, tmax, h_tab[1], h_tab[0][lmax + 1])) {
+  {
+    if (wcorr_eligible(tmax, h_tab[1], h_tab[0][lmax + 1])) {
       WCTable w;
       std::memset(&w, 0, sizeof w);
       w.lmax = lmax;
@@ -739,23 +811,23 @@ static cudaError_t wilson_gf_t(const void *links, const Geom &g, const int *cons
         w.R = g.L[nu] < WC_RO ? g.L[nu] : WC_RO;
         w.ntile_rows = (g.L[nu] + w.R - 1) / w.R;
         w.ntiles = ((c.ncols + WC_CW - 1) / WC_CW) * w.ntile_rows;
-        const size_t smem = wcorr_smem<N>(npairs);
+        const size_t smem = wcorr_smem<N, T>(npairs);
         // the attribute is per device: set it on every launch
-        cudaFuncSetAttribute(wcorr_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
-        static int per_sm[4] = {0, 0, 0, 0};
-        static int sms = 0;
-        if (!per_sm[N]) {
+        cudaFuncSetAttribute(wcorr_kernel<N, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 112 * 1024);
+        static int per_sm = 0, sms = 0;  // one instance per (N, T)
+        if (!per_sm) {
           int dev = 0;
           cudaGetDevice(&dev);
           cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
           int nb = 0;
-          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, wcorr_kernel<N>, WC_THREADS, wcorr_smem<N>(WL_MAXP));
-          per_sm[N] = nb > 0 ? nb : 1;
+          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, wcorr_kernel<N, T>, WC_THREADS,
+                                                        wcorr_smem<N, T>(WL_MAXP));
           if (sms <= 0) sms = 148;
+          per_sm = nb > 0 ? nb : 1;
         }
-        const long long want = (long long)sms * per_sm[N];
+        const long long want = (long long)sms * per_sm;
         const int grid = (int)std::min<long long>(std::min<long long>(want, nblk), w.ntiles > 0 ? w.ntiles : 1);
-        wcorr_kernel<N><<<grid, WC_THREADS, smem, st>>>(up, c, w, tmax, d_part);
+        wcorr_kernel<N, T><<<grid, WC_THREADS, smem, st>>>(up, c, w, tmax, d_part);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
         *grid_used = grid;

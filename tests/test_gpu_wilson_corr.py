@@ -1,7 +1,7 @@
-"""Column-correlation Wilson-loop kernel (FP32 links, every T in 1..8) against
-the oracle: colour groups, tiles that do not divide the nu axis, short axes,
-loops that wrap the lattice along mu, partial T lists, and the tables that
-stay on the entry-per-origin kernel (T > 8, repeated pairs)."""
+"""Column-correlation Wilson-loop kernel (every T in 1..8, FP32 and FP64
+links) against the oracle: colour groups, tiles that do not divide the nu
+axis, short axes, loops that wrap the lattice along mu, partial T lists, and
+the tables that stay on the entry-per-origin kernel (T > 8, repeated pairs)."""
 import numpy as np
 import pytest
 
@@ -11,39 +11,41 @@ from oracle.oracle import Lat
 pytestmark = pytest.mark.gpu
 
 ATOL = 2e-6  # FP32 links: per-site traces in FP32, sums in FP64
+TOL = {"mixed": dict(rtol=0, atol=ATOL), "fp64": dict(rtol=1e-12, atol=1e-14)}
 
 
-def field(oracle, nc, L, seed):
+def field(oracle, nc, L, seed, precision="mixed"):
     lat = Lat(nc, L)
     U = oracle.init(lat, True, seed)
-    g = GaugeField(L, nc, "mixed")
+    g = GaugeField(L, nc, precision)
     g.upload(U)
     return lat, U, g
 
 
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
 @pytest.mark.parametrize("nc", [1, 2, 3])
 @pytest.mark.parametrize("L", [[4, 4, 4, 4], [6, 4, 2, 10], [4, 6, 4, 36], [6, 4, 20], [10, 6], [4, 2, 2, 70]])
-def test_temporal_loops_match_oracle(oracle, nc, L):
-    lat, U, g = field(oracle, nc, L, 31 + nc)
+def test_temporal_loops_match_oracle(oracle, nc, L, precision):
+    lat, U, g = field(oracle, nc, L, 31 + nc, precision)
     pairs = [(l, t) for l in range(1, 10) for t in range(1, 9)]
-    np.testing.assert_allclose(g.wilson_loop_temporal(pairs), oracle.wilson_temporal(lat, U, pairs), rtol=0,
-                               atol=ATOL)
+    np.testing.assert_allclose(g.wilson_loop_temporal(pairs), oracle.wilson_temporal(lat, U, pairs),
+                               **TOL[precision])
     g.close()
 
 
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
 @pytest.mark.parametrize("nc", [2, 3])
-def test_partial_t_lists_and_other_planes(oracle, nc):
+def test_partial_t_lists_and_other_planes(oracle, nc, precision):
     L = [6, 4, 8, 12]
-    lat, U, g = field(oracle, nc, L, 41)
+    lat, U, g = field(oracle, nc, L, 41, precision)
+    tol = TOL[precision]
     pairs = [(3, 2), (1, 5), (7, 1), (2, 8), (5, 3)]  # tmax 8 with gaps; L in any order
-    np.testing.assert_allclose(g.wilson_loop_temporal(pairs), oracle.wilson_temporal(lat, U, pairs), rtol=0,
-                               atol=ATOL)
+    np.testing.assert_allclose(g.wilson_loop_temporal(pairs), oracle.wilson_temporal(lat, U, pairs), **tol)
     short = [(2, 1), (4, 3), (1, 2)]  # tmax 3
-    np.testing.assert_allclose(g.wilson_loop_temporal(short), oracle.wilson_temporal(lat, U, short), rtol=0,
-                               atol=ATOL)
+    np.testing.assert_allclose(g.wilson_loop_temporal(short), oracle.wilson_temporal(lat, U, short), **tol)
     for mu, nu in [(3, 0), (0, 2), (2, 1)]:
         np.testing.assert_allclose(g.wilson_loop_mu_nu(mu, nu, pairs), oracle.wilson_mu_nu(lat, U, mu, nu, pairs),
-                                   rtol=0, atol=ATOL)
+                                   **tol)
     g.close()
 
 
