@@ -814,18 +814,15 @@ static cudaError_t wilson_gf_t(const void *links, const Geom &g, const int *cons
         const size_t smem = wcorr_smem<N, T>(npairs);
         // the attribute is per device: set it on every launch
         cudaFuncSetAttribute(wcorr_kernel<N, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 112 * 1024);
-        static int per_sm = 0, sms = 0;  // one instance per (N, T)
-        if (!per_sm) {
-          int dev = 0;
+        // resident CTAs on the device, queried once per (N, T) (thread-safe static initialisation)
+        static const long long want = [] {
+          int dev = 0, sms = 0, nb = 0;
           cudaGetDevice(&dev);
           cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-          int nb = 0;
           cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, wcorr_kernel<N, T>, WC_THREADS,
                                                         wcorr_smem<N, T>(WL_MAXP));
-          if (sms <= 0) sms = 148;
-          per_sm = nb > 0 ? nb : 1;
-        }
-        const long long want = (long long)sms * per_sm;
+          return (long long)(sms > 0 ? sms : 148) * (nb > 0 ? nb : 1);
+        }();
         const int grid = (int)std::min<long long>(std::min<long long>(want, nblk), w.ntiles > 0 ? w.ntiles : 1);
         wcorr_kernel<N, T><<<grid, WC_THREADS, smem, st>>>(up, c, w, tmax, d_part);
         cudaError_t e = cudaGetLastError();
