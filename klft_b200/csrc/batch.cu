@@ -376,6 +376,8 @@ klft_status enqueue_multi_sweep(const std::vector<SweepItem> &items, unsigned lo
     d.ctr = lat->d_counters;
     d.g = lat->g;
     d.a = it.a;
+    if (key.dtype == 0 && key.exp && !(d.a.bm = bm_table()))
+      return fail(KLFT_ECUDA, "enqueue_multi_sweep: Box-Muller table unavailable");
     d.df = it.df;
     d.index = it.acc_index >= 0 ? it.acc_index : i;
     d.block_begin = grp->blocks.back();

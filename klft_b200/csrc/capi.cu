@@ -220,6 +220,9 @@ klft_status klft_lattice_create(int nc, int ndims, const int *L, int precision, 
     e = launch_init(nc, precision == KLFT_PRECISION_FP64 ? 0 : 1, lat->links, g, start == KLFT_START_HOT, seed, 0,
                     lat->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(lat->stream);
+  // the FP64 SU(3) exp proposal's Box-Muller table, built here so that no
+  // sweep (captured into a graph or not) has to allocate it
+  if (e == cudaSuccess && nc == 3 && precision == KLFT_PRECISION_FP64 && !bm_table()) e = cudaErrorMemoryAllocation;
   if (e != cudaSuccess) {
     klft_status s = cuda_fail(e, "klft_lattice_create");
     klft_lattice_destroy(lat);

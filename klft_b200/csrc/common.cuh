@@ -222,25 +222,49 @@ template <int N, typename T, typename A> KLFT_HD A retr_nd(const Mat<N, T> &a, c
 template <typename T> KLFT_HD Mat<1, T> restore(const Mat<1, T> &a) {
   Mat<1, T> c;
   const T n = sqrt(a.e[0][0].re * a.e[0][0].re + a.e[0][0].im * a.e[0][0].im);
-  c.e[0][0] = cdiv(a.e[0][0], n);
+  if constexpr (sizeof(T) == 4) {
+    const T i = T(1) / n;  // FP32: one reciprocal (see the SU(3) form)
+    c.e[0][0] = mk<T>(a.e[0][0].re * i, a.e[0][0].im * i);
+  } else {
+    c.e[0][0] = cdiv(a.e[0][0], n);
+  }
   return c;
 }
 template <typename T> KLFT_HD Mat<2, T> restore(const Mat<2, T> &a) {
   Mat<2, T> c;
   const T n = sqrt(a.e[0][0].re * a.e[0][0].re + a.e[0][0].im * a.e[0][0].im + a.e[0][1].re * a.e[0][1].re +
                    a.e[0][1].im * a.e[0][1].im);
+  if constexpr (sizeof(T) == 4) {
+    const T r = T(1) / n;  // FP32: one reciprocal (see the SU(3) form)
 #pragma unroll
-  for (int i = 0; i < 2; ++i)
+    for (int i = 0; i < 2; ++i)
 #pragma unroll
-    for (int j = 0; j < 2; ++j) c.e[i][j] = cdiv(a.e[i][j], n);
+      for (int j = 0; j < 2; ++j) c.e[i][j] = mk<T>(a.e[i][j].re * r, a.e[i][j].im * r);
+  } else {
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+      for (int j = 0; j < 2; ++j) c.e[i][j] = cdiv(a.e[i][j], n);
+  }
   return c;
 }
 template <typename T> KLFT_HD Mat<3, T> restore(const Mat<3, T> &a) {
   Mat<3, T> c;
   const T n0 = sqrt((conj(a.e[0][0]) * a.e[0][0] + conj(a.e[0][1]) * a.e[0][1] + conj(a.e[0][2]) * a.e[0][2]).re);
   const T n1 = sqrt((conj(a.e[1][0]) * a.e[1][0] + conj(a.e[1][1]) * a.e[1][1] + conj(a.e[1][2]) * a.e[1][2]).re);
+  if constexpr (sizeof(T) == 4) {
+    // FP32: one reciprocal per row (the mixed form has no reference arithmetic
+    // to follow; six IEEE divisions per row cost ~3 % of an exp-proposal sweep)
+    const T i0 = T(1) / n0, i1 = T(1) / n1;
 #pragma unroll
-  for (int j = 0; j < 3; ++j) { c.e[0][j] = cdiv(a.e[0][j], n0); c.e[1][j] = cdiv(a.e[1][j], n1); }
+    for (int j = 0; j < 3; ++j) {
+      c.e[0][j] = mk<T>(a.e[0][j].re * i0, a.e[0][j].im * i0);
+      c.e[1][j] = mk<T>(a.e[1][j].re * i1, a.e[1][j].im * i1);
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < 3; ++j) { c.e[0][j] = cdiv(a.e[0][j], n0); c.e[1][j] = cdiv(a.e[1][j], n1); }
+  }
   c.e[2][0] = conj(c.e[0][1] * c.e[1][2] - c.e[0][2] * c.e[1][1]);
   c.e[2][1] = conj(c.e[0][2] * c.e[1][0] - c.e[0][0] * c.e[1][2]);
   c.e[2][2] = conj(c.e[0][0] * c.e[1][1] - c.e[0][1] * c.e[1][0]);

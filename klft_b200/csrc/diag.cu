@@ -53,13 +53,13 @@ KLFT_D Mat<3, float> to_mixed(const Mat<3, double> &u) {
 // largest |d| as the bits of a non-negative double.
 __global__ void __launch_bounds__(128) dS_error_kernel(Links<3, double> U, Geom g, double beta, double eps, int nhits,
                                                        uint64_t seed, uint64_t chain, uint32_t sweep, double *acc,
-                                                       unsigned long long *dmax) {
+                                                       unsigned long long *dmax, const double *bm) {
   const long long lin = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   double loc[6] = {0, 0, 0, 0, 0, 0};
   double m = 0.0;
   if (lin < g.V) {
     const Site x = site_from_lin(g, lin);
-    const ExpHitStream hs{(uint32_t)seed, (uint32_t)(seed >> 32) ^ (uint32_t)chain, site_lex(g, x), sweep};
+    const ExpHitStream hs{(uint32_t)seed, (uint32_t)(seed >> 32) ^ (uint32_t)chain, site_lex(g, x), sweep, bm};
     for (int mu = 0; mu < g.nd; ++mu) {
       // staple in FP64, and in FP32 from the mixed form's links
       Mat<3, double> S64 = mzero<3, double>();
@@ -134,10 +134,12 @@ extern "C" klft_status klft_exp_proposal_dS_error(klft_lattice *lat, double beta
   uint32_t sweep = 0;
   CK(cudaMemcpyAsync(&sweep, lat->d_counters, sizeof sweep, cudaMemcpyDeviceToHost, lat->stream));
   CK(cudaStreamSynchronize(lat->stream));
+  const double *bm = bm_table();
+  if (!bm) return fail(KLFT_ECUDA, "klft_exp_proposal_dS_error: Box-Muller table unavailable");
   const unsigned grid = (unsigned)((lat->g.V + 127) / 128);
   dS_error_kernel<<<grid, 128, 0, lat->stream>>>(Links<3, double>{(cx<double> *)lat->links, lat->g.V}, lat->g, beta,
                                                  eps, nhits, lat->seed, lat->chain, sweep, d_acc,
-                                                 (unsigned long long *)(d_acc + 6));
+                                                 (unsigned long long *)(d_acc + 6), bm);
   CK(cudaGetLastError());
   double h[8];
   CK(cudaMemcpyAsync(h, d_acc, sizeof h, cudaMemcpyDeviceToHost, lat->stream));

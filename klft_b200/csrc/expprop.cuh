@@ -175,13 +175,16 @@ template <typename V> KLFT_D XMat<V> expi_gellmann(const V h[8], V s) {
 
 // Box-Muller pair from the two 16-bit halves of one stream word,
 // u = (k + 1/2) 2^-16; (r cos 2 pi u_b, r sin 2 pi u_b), r = sqrt(-2 ln u_a).
-KLFT_D void box_muller16(uint32_t w, double &g0, double &g1) {
-  const double ua = ((double)(w & 0xFFFFu) + 0.5) * 0x1.0p-16, ub = ((double)(w >> 16) + 0.5) * 0x1.0p-16;
-  const double r = sqrt(-2.0 * log(ua));
-  double sn, cs;
-  sincospi(2.0 * ub, &sn, &cs);
-  g0 = r * cs;
-  g1 = r * sn;
+// FP64: each half takes one of 2^16 values, so r, cos and sin are read from a
+// table built on the host (bm_table(): r at [k], (cos, sin) at 2^16 + 2 k), the
+// same expressions the oracle evaluates, instead of FP64 log / sqrt / sincos on
+// the device (those cost about 30 % of an FP64 sweep).
+constexpr int BM_TAB = 1 << 16;
+KLFT_D void box_muller16(uint32_t w, double &g0, double &g1, const double *bm) {
+  const double r = __ldg(bm + (w & 0xFFFFu));
+  const double2 cs = __ldg((const double2 *)(bm + BM_TAB) + (w >> 16));
+  g0 = r * cs.x;
+  g1 = r * cs.y;
 }
 // FP32: the halves become floats in [1, 2) through their bit patterns (exact),
 // SFU log, rsqrt and sincos; cos/sin(2 pi u) = -cos/sin(2 pi (u - 1/2)) keeps
@@ -200,6 +203,7 @@ KLFT_D void box_muller16(uint32_t w, float &g0, float &g1) {
 // Stream positions of the exp(i eps H) proposal of one site and sweep.
 struct ExpHitStream {
   uint32_t k0, k1, site, step;
+  const double *bm;  // Box-Muller table of the FP64 form (bm_table()); unused in FP32
   KLFT_D void block(uint32_t b, uint32_t w[4], uint32_t sub = 0) const {
     w[0] = b; w[1] = site; w[2] = step; w[3] = (KIND_METROPOLIS << 24) | sub;
     philox4x32_10(w, k0, k1);
@@ -209,7 +213,10 @@ struct ExpHitStream {
     uint32_t w[4];
     block(h, w);
 #pragma unroll
-    for (int k = 0; k < 4; ++k) box_muller16(w[k], g[2 * k], g[2 * k + 1]);
+    for (int k = 0; k < 4; ++k) {
+      if constexpr (sizeof(T) == 8) box_muller16(w[k], g[2 * k], g[2 * k + 1], bm);
+      else box_muller16(w[k], g[2 * k], g[2 * k + 1]);
+    }
   }
   KLFT_D void accept_block(uint32_t h, uint32_t w[4]) const { block(h >> 2, w, 1); }
 };

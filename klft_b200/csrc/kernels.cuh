@@ -10,7 +10,13 @@ struct MetroArgs {
   double beta, delta, eps;
   int nhits, proposal;
   uint64_t seed, chain;
+  const double *bm = nullptr;  // FP64 Box-Muller table (bm_table()), set at launch
 };
+
+// The FP64 Box-Muller table of the current device (BM_TAB radii, then BM_TAB
+// (cos, sin) pairs, 1.5 MB), built on the host and uploaded on first use; call
+// it outside stream capture (lattice creation does).  Null on a CUDA error.
+const double *bm_table();
 
 // Launches per sweep: 2 Nd link passes for the SU(3) exp(i eps H) proposal
 // (proposal 1), else the reference's 2^Nd site classes.

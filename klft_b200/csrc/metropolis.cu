@@ -75,6 +75,12 @@ cudaError_t launch_metropolis_pass(int nc, int dtype, void *links, const Geom &g
                                    const uint32_t *d_sweep, unsigned long long *d_nacc, const Defect &df, int block,
                                    cudaStream_t st) {
   if (dtype == 0) {
+    if (nc == 3 && a.proposal == 1) {
+      // the FP64 exp(i eps H) proposal reads its Gaussians from the host-built table
+      MetroArgs b = a;
+      if (!(b.bm = bm_table())) return cudaErrorMemoryAllocation;
+      return launch_nd<3, double>(g.nd, links, g, val, b, d_sweep, d_nacc, df, block, st);
+    }
     switch (nc) {
       case 1: return launch_nd<1, double>(g.nd, links, g, val, a, d_sweep, d_nacc, df, block, st);
       case 2: return launch_nd<2, double>(g.nd, links, g, val, a, d_sweep, d_nacc, df, block, st);

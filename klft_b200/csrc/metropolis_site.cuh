@@ -206,7 +206,7 @@ KLFT_D int link_update_exp(const Links<3, T> &U, const Geom &g, const Site &x, i
                            uint32_t sweep, const Defect &df) {
   if (open_link(g, x, mu)) return 0;
   int nacc = 0;
-  const ExpHitStream hs{(uint32_t)a.seed, (uint32_t)(a.seed >> 32) ^ (uint32_t)a.chain, site_lex(g, x), sweep};
+  const ExpHitStream hs{(uint32_t)a.seed, (uint32_t)(a.seed >> 32) ^ (uint32_t)a.chain, site_lex(g, x), sweep, a.bm};
   const long long lx = site_lin(g, x);
   const T bnc = (T)a.beta / T(3);
   const T half_eps = (T)(0.5 * a.eps);
