@@ -413,12 +413,10 @@ klft_status klft_wilson_loop_temporal(klft_lattice *lat, const int *pairs, int n
   const size_t nsum = (size_t)(nd - 1) * npairs;
   CK(lat->s_out.ensure((nsum > KLFT_RESULT_SLOTS ? nsum : KLFT_RESULT_SLOTS) * sizeof(double)));
   WilsonPlan plan;
-  klft_status s = make_wilson_plan(lat, pairs, npairs, nd - 1, plan);
+  klft_status s = make_wilson_plan(lat, pairs, npairs, nd - 1, plan, 0, nd - 1);
   if (s != KLFT_OK) return s;
-  for (int mu = 0; mu < nd - 1; ++mu) {
-    s = enqueue_wilson_plane(lat, plan, mu, nd - 1, mu > 0, (double *)lat->s_out.ptr + (size_t)mu * npairs);
-    if (s != KLFT_OK) return s;
-  }
+  s = enqueue_wilson_spatial(lat, plan, false, (double *)lat->s_out.ptr, npairs);
+  if (s != KLFT_OK) return s;
   std::vector<double> sums(nsum);
   CK(cudaMemcpyAsync(sums.data(), lat->s_out.ptr, nsum * sizeof(double), cudaMemcpyDeviceToHost, lat->stream));
   CK(cudaStreamSynchronize(lat->stream));
@@ -488,7 +486,7 @@ klft_status klft_run_cycles(klft_lattice *lat, double beta, double delta, int nh
   double *d_w = d_plaq + ncycles;
   WilsonPlan plan;
   if (npairs > 0) {
-    klft_status s = make_wilson_plan(lat, temporal_pairs, npairs, nd - 1, plan);
+    klft_status s = make_wilson_plan(lat, temporal_pairs, npairs, nd - 1, plan, 0, nd - 1);
     if (s != KLFT_OK) return s;
   }
   CK(cudaMemsetAsync(d_nacc, 0, (size_t)ncycles * sizeof(unsigned long long), lat->stream));
@@ -515,9 +513,9 @@ klft_status klft_run_cycles(klft_lattice *lat, double beta, double delta, int nh
       CK(launch_plaquette(lat->nc, lat->dtype(), lat->links, lat->g, (double *)lat->s_part.ptr, nblk, d_plaq + c,
                           lat->stream, plaq_nu_end));
     }
-    for (int mu = 0; mu < nd - 1 && npairs > 0; ++mu) {
-      // the axial-gauge transformation along nu = Nd-1 is shared by the spatial planes
-      s = enqueue_wilson_plane(lat, plan, mu, nd - 1, mu > 0, d_w + (size_t)c * nw + (size_t)mu * npairs);
+    if (npairs > 0) {
+      // the spatial planes share the axial-gauge transformation along nu = Nd-1
+      s = enqueue_wilson_spatial(lat, plan, false, d_w + (size_t)c * nw, npairs);
       if (s != KLFT_OK) return s;
     }
   }
@@ -627,8 +625,8 @@ klft_status klft_run_metropolis(klft_lattice *lat, double beta, double delta, in
       CK(launch_plaquette(lat->nc, lat->dtype(), lat->links, lat->g, (double *)lat->s_part.ptr,
                           plaquette_blocks(lat->g), slot, lat->stream));
     int last_nu = -1;
-    for (int mu = 0; mu < nd - 1 && ntw > 0; ++mu) {
-      s = enqueue_wilson_plane(lat, tplan, mu, nd - 1, last_nu == nd - 1, slot + 1 + (size_t)mu * ntemporal);
+    if (ntw > 0) {
+      s = enqueue_wilson_spatial(lat, tplan, false, slot + 1, ntemporal);
       if (s != KLFT_OK) return s;
       last_nu = nd - 1;
     }
@@ -750,7 +748,7 @@ double normalize_wilson(const klft_lattice *lat, double sum) {
 // and, for the gauge-fixed form, the (T, pair) lists per loop length L.  All
 // scratch the plane kernels need is sized here, before anything is enqueued.
 klft_status make_wilson_plan(klft_lattice *lat, const int *pairs, int npairs, int nu, WilsonPlan &plan,
-                             size_t tab_off) {
+                             size_t tab_off, int nplanes) {
   plan = WilsonPlan();
   plan.npairs = npairs;
   plan.tab_off = tab_off;
@@ -775,14 +773,14 @@ klft_status make_wilson_plan(klft_lattice *lat, const int *pairs, int npairs, in
         }
     }
     plan.off[plan.lmax + 1] = (int)plan.T.size();
-    CK(lat->s_gf.ensure(wilson_gf_scratch(lat->nc, lat->dtype(), lat->g, nu, plan.tmax)));
+    CK(lat->s_gf.ensure(wilson_gf_scratch(lat->nc, lat->dtype(), lat->g, nu, plan.tmax, nplanes)));
   }
   CK(lat->s_tab.ensure((tab_off + h.size()) * sizeof(int) + 16));
   CK(cudaMemcpyAsync((int *)lat->s_tab.ptr + tab_off, h.data(), h.size() * sizeof(int), cudaMemcpyHostToDevice,
                      lat->stream));
   CK(cudaStreamSynchronize(lat->stream));  // h is pageable and local
   const int nblk = plan.gf ? wilson_gf_blocks(lat->g) : plaquette_blocks(lat->g);
-  CK(lat->s_part.ensure((size_t)nblk * (npairs > 1 ? npairs : 1) * sizeof(double)));
+  CK(lat->s_part.ensure((size_t)nblk * (npairs > 1 ? npairs : 1) * (size_t)nplanes * sizeof(double)));
   return KLFT_OK;
 }
 
@@ -792,13 +790,36 @@ klft_status enqueue_wilson_plane(klft_lattice *lat, const WilsonPlan &plan, int 
   const int *tab = (const int *)lat->s_tab.ptr + plan.tab_off;
   if (plan.gf) {
     const int *ht[3] = {plan.off.data(), plan.T.data(), plan.p.data()};
-    CK(launch_wilson_gf(lat->nc, lat->dtype(), lat->links, lat->g, mu, nu, ht, plan.lmax, plan.tmax, plan.npairs,
-                        omega_ready, lat->s_gf.ptr, (double *)lat->s_part.ptr, wilson_gf_blocks(lat->g), d_out,
-                        lat->stream));
+    CK(launch_wilson_gf(lat->nc, lat->dtype(), lat->links, lat->g, &mu, 1, nu, ht, plan.lmax, plan.tmax,
+                        plan.npairs, omega_ready, lat->s_gf.ptr, (double *)lat->s_part.ptr, wilson_gf_blocks(lat->g),
+                        d_out, plan.npairs, lat->stream));
   } else {
     const int nblk = plaquette_blocks(lat->g);
     CK(launch_wilson_direct(lat->nc, lat->dtype(), lat->links, lat->g, mu, nu, tab, plan.npairs,
                             (double *)lat->s_part.ptr, nblk, d_out, lat->stream));
+  }
+  return KLFT_OK;
+}
+
+// enqueue the planes (mu, Nd-1), mu < Nd-1, of a plan made with nplanes = Nd-1:
+// d_out[mu * out_stride + k] = unnormalised sum for pair k; the gauge-fixed form
+// runs all planes in one loop-kernel launch (one tile queue, so the last wave of
+// one plane does not idle while the next plane waits for its own launch).
+klft_status enqueue_wilson_spatial(klft_lattice *lat, const WilsonPlan &plan, bool omega_ready, double *d_out,
+                                   int out_stride) {
+  const int nu = lat->g.nd - 1;
+  if (plan.gf) {
+    const int *ht[3] = {plan.off.data(), plan.T.data(), plan.p.data()};
+    int mus[3] = {0, 1, 2};
+    // planes mu = 0 .. nu - 1
+    CK(launch_wilson_gf(lat->nc, lat->dtype(), lat->links, lat->g, mus, nu, nu, ht, plan.lmax, plan.tmax,
+                        plan.npairs, omega_ready, lat->s_gf.ptr, (double *)lat->s_part.ptr, wilson_gf_blocks(lat->g),
+                        d_out, out_stride, lat->stream));
+    return KLFT_OK;
+  }
+  for (int mu = 0; mu < nu; ++mu) {
+    klft_status s = enqueue_wilson_plane(lat, plan, mu, nu, omega_ready || mu > 0, d_out + (size_t)mu * out_stride);
+    if (s != KLFT_OK) return s;
   }
   return KLFT_OK;
 }

@@ -128,9 +128,12 @@ struct WilsonPlan {
 };
 // tab_off: where the pairs go in lat->s_tab (several plans in flight at once
 // use disjoint ranges; the caller then sizes s_tab for all of them first)
+// nplanes: the planes one enqueue_wilson_spatial call covers (scratch for one U' each)
 klft_status make_wilson_plan(klft_lattice *lat, const int *pairs, int npairs, int nu, WilsonPlan &plan,
-                             size_t tab_off = 0);
+                             size_t tab_off = 0, int nplanes = 1);
 klft_status enqueue_wilson_plane(klft_lattice *lat, const WilsonPlan &plan, int mu, int nu, bool omega_ready,
                                  double *d_out);
+klft_status enqueue_wilson_spatial(klft_lattice *lat, const WilsonPlan &plan, bool omega_ready, double *d_out,
+                                   int out_stride);
 klft_status wilson_sums(klft_lattice *lat, int mu, int nu, const int *pairs, int npairs, double *sums);
 }  // namespace klft

@@ -56,15 +56,20 @@ cudaError_t launch_wilson_direct(int nc, int dtype, const void *links, const Geo
                                  cudaStream_t st);
 
 // Wilson loops of a pair list in the (mu, nu) plane by axial gauge fixing (wilson.cu)
-size_t wilson_gf_scratch(int nc, int dtype, const Geom &g, int nu, int tmax);
+// scratch of the gauge-fixed loops of nplanes planes sharing nu (one Omega, one U' per plane)
+size_t wilson_gf_scratch(int nc, int dtype, const Geom &g, int nu, int tmax, int nplanes = 1);
 size_t wilson_gf_smem(int nc, int dtype, const Geom &g, int nu, int tmax, int npairs);
 int wilson_gf_blocks(const Geom &g);
 // h_tab = {off[lmax+2], T[npairs], p[npairs]} on the host (passed in the kernel
 // parameters); npairs, lmax <= WL_MAXP
 constexpr int WL_MAXP = 128;
-cudaError_t launch_wilson_gf(int nc, int dtype, const void *links, const Geom &g, int mu, int nu,
-                             const int *const *h_tab, int lmax, int tmax, int npairs, bool omega_ready,
-                             void *scratch, double *d_part, int nblk, double *d_out, cudaStream_t st);
+// Loops of the planes (mus[i], nu), i < nplanes <= 3, sharing one axial-gauge
+// transformation; plane i's sums go to d_out[i * out_stride + k]; d_part holds
+// nblk * npairs * nplanes doubles.
+cudaError_t launch_wilson_gf(int nc, int dtype, const void *links, const Geom &g, const int *mus, int nplanes,
+                             int nu, const int *const *h_tab, int lmax, int tmax, int npairs, bool omega_ready,
+                             void *scratch, double *d_part, int nblk, double *d_out, int out_stride,
+                             cudaStream_t st);
 
 int plaquette_blocks(const Geom &g);
 // ordered final reduction of nblk partials for each of n outputs

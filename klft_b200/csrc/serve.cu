@@ -158,8 +158,9 @@ uint64_t footprint_of(const klft_job &j) {
   if (j.n_wilson > 0) {
     int tmax = 0;
     for (int k = 0; k < j.n_wilson; ++k) tmax = std::max(tmax, j.wilson_pairs[2 * k + 1]);
-    b += wilson_gf_scratch(j.nc, dtype, g, j.ndims - 1, tmax);
-    b += (uint64_t)std::max(wilson_gf_blocks(g), plaquette_blocks(g)) * j.n_wilson * sizeof(double) + 4096;
+    b += wilson_gf_scratch(j.nc, dtype, g, j.ndims - 1, tmax, j.ndims - 1);
+    b += (uint64_t)std::max(wilson_gf_blocks(g), plaquette_blocks(g)) * j.n_wilson * (j.ndims - 1) * sizeof(double) +
+         4096;
   }
   if (j.kind == KLFT_JOB_HMC) b += hmc_footprint(j.nc, dtype, g, std::max(j.ntraj, 1));
   return b;
@@ -301,7 +302,8 @@ void klft_server::admit(std::unique_ptr<Job> jp) {
   ck(lat->s_out.ensure(KLFT_RESULT_SLOTS * sizeof(double)), "result slots");
   ck(lat->s_part.ensure((size_t)plaquette_blocks(lat->g) * sizeof(double)), "partials");
   ck(cudaEventCreateWithFlags(&j.ev, cudaEventDisableTiming), "cudaEventCreate");
-  if (s == KLFT_OK && j.d.n_wilson > 0) s = make_wilson_plan(lat, j.d.wilson_pairs, j.d.n_wilson, j.d.ndims - 1, j.plan);
+  if (s == KLFT_OK && j.d.n_wilson > 0)
+    s = make_wilson_plan(lat, j.d.wilson_pairs, j.d.n_wilson, j.d.ndims - 1, j.plan, 0, j.d.ndims - 1);
   if (s == KLFT_OK && j.d.kind == KLFT_JOB_HMC) {
     s = hmc_prepare(lat, std::max(j.d.ntraj, 1));
     for (cudaEvent_t &e : j.tev) ck(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
@@ -340,9 +342,9 @@ void klft_server::start_measure(Job &j, cudaEvent_t after) {
       s = enqueue_plaquette(lat, kSlotPlaq);
       launches += 2;
     }
-    for (int mu = 0; s == KLFT_OK && j.d.n_wilson > 0 && mu < j.d.ndims - 1; ++mu) {
-      s = enqueue_wilson_plane(lat, j.plan, mu, j.d.ndims - 1, mu > 0, d_out + kSlotWilson + mu * KLFT_JOB_MAX_WILSON);
-      launches += 3;
+    if (s == KLFT_OK && j.d.n_wilson > 0) {
+      s = enqueue_wilson_spatial(lat, j.plan, false, d_out + kSlotWilson, KLFT_JOB_MAX_WILSON);
+      launches += 2 * (j.d.ndims - 1) + 2;  // omega, U' per plane, the loop kernel, a reduction per plane
     }
     if (s == KLFT_OK && j.d.kind == KLFT_JOB_HMC) {
       s = hmc_enqueue_summary(lat, j.d.ntraj, d_out + kSlotHmc);

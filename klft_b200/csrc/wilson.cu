@@ -219,8 +219,9 @@ __global__ void __launch_bounds__(32 * UP_RB) uprime_kernel(Links<N, T> U, Geom 
                                                             CField<N, T> pol, CField<N, T> up) {
   __shared__ cx<T> tile[N * N][UP_RB][33];
   const long long nct = (c.ncols + 31) / 32;
-  const long long ctile = blockIdx.x % nct;
-  const int row0 = (int)(blockIdx.x / nct) * UP_RB;
+  const unsigned bq = blockIdx.x / (unsigned)nct;  // the grid has fewer than 2^32 blocks
+  const long long ctile = blockIdx.x - bq * (unsigned)nct;
+  const int row0 = (int)bq * UP_RB;
   const int cl = threadIdx.x & 31, r = threadIdx.x >> 5;
   const long long col = ctile * 32 + cl;
   const int row = row0 + r;
@@ -416,12 +417,12 @@ __global__ void __launch_bounds__(WL_THREADS, WLMinBlocks<T>::v)
   const int ebase = cc * 2 * half;
   const int eo0 = ebase + q, eo1 = ebase + half + q;  // slots of the origin rows 2q, 2q + 1
   for (long long tile = blockIdx.x; tile < w.ntiles; tile += gridDim.x) {
-    const long long ctile = tile / w.ntile_rows;
+    const long long ctile = (long long)((unsigned)tile / (unsigned)w.ntile_rows);  // V < 2^31: 32-bit
     const int r0 = (int)(tile - ctile * w.ntile_rows) * w.R;
     const long long col = ctile * w.CW + cc;
     const bool col_ok = has_origin && col < c.ncols;
     // coordinate of the column along mu; colL = column of x + (L-1) mu, stepped per L
-    const int xm = col_ok ? (int)((col / c.csmu) % c.Lmu) : 0;
+    const int xm = col_ok ? (int)(((unsigned)col / (unsigned)c.csmu) % (unsigned)c.Lmu) : 0;
     long long colL = col;
     int xl = xm;
     Mat<N, T> own0, own1;  // S'_L at rows r0 + 2q and r0 + 2q + 1
@@ -550,9 +551,16 @@ template <int N, typename T> struct WCCol {
 // consumer work per column: component k of origin chunk c, NCH chunks of 32 / NCH rows
 template <int N> struct WCChunks { static constexpr int v = N == 3 ? 1 : N == 2 ? 2 : 8; };
 
+// Up to WC_MAXPL planes (mu_i, nu) sharing nu in one launch: the tiles of plane
+// i follow those of plane i - 1, and its U' starts pstride entries after
+// plane i - 1's.
+constexpr int WC_MAXPL = 3;
 struct WCTable {
   int lmax, npairs, R, ntile_rows;
-  long long ntiles;
+  long long ntiles1;  // tiles per plane
+  int nplanes;
+  long long pstride;
+  int mu[WC_MAXPL], csmu[WC_MAXPL], Lmu[WC_MAXPL];
   short pm[WL_MAXP + 1][WC_TW];  // pair index of (L, T = j + 1), or -1
 };
 
@@ -630,33 +638,41 @@ __global__ void __launch_bounds__(WC_THREADS, WCMinBlocks<T>::v)
   static_assert(KC * NCH <= WC_PT, "consumer tasks must fit the threads of a column");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T *buf = (T *)smem_raw;                                   // [2][WC_CW][CS]
-  double *acc = (double *)(buf + 2 * WC_CW * CS);          // [npairs][WC_WARPS]
+  double *acc = (double *)(buf + 2 * WC_CW * CS);          // [nplanes * npairs][WC_WARPS]
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int cc = tid / WC_PT, q = tid % WC_PT;
-  for (int i = tid; i < 2 * WC_CW * CS; i += WC_THREADS) buf[i] = 0.f;  // rows never written stay finite
-  for (int p = tid; p < w.npairs * WC_WARPS; p += WC_THREADS) acc[p] = 0.0;
+  for (int i = tid; i < 2 * WC_CW * CS; i += WC_THREADS) buf[i] = T(0);  // rows never written stay finite
+  const int nout = w.nplanes * w.npairs;
+  for (int p = tid; p < nout * WC_WARPS; p += WC_THREADS) acc[p] = 0.0;
   const bool consumer = q < KC * NCH;
   const int kq = q % KC, ob = (q / KC) * NO;  // consumer's component and first origin row
   int stage = 0;
   __syncthreads();
-  for (long long tile = blockIdx.x; tile < w.ntiles; tile += gridDim.x) {
-    const long long ctile = tile / w.ntile_rows;
-    const int r0 = (int)(tile - ctile * w.ntile_rows) * w.R;
+  const long long ntiles = w.ntiles1 * w.nplanes;
+  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    // V < 2^31: tiles and columns in 32-bit arithmetic
+    const int pl = (int)((unsigned)tile / (unsigned)w.ntiles1);
+    const unsigned t1 = (unsigned)tile - (unsigned)pl * (unsigned)w.ntiles1;
+    const long long ctile = (long long)(t1 / (unsigned)w.ntile_rows);
+    const int r0 = (int)(t1 - (unsigned)ctile * (unsigned)w.ntile_rows) * w.R;
     const int reff = min(w.R, c.Lnu - r0);  // origin rows of this tile
     const int rneed = reff + tmax;           // rows read as origins or partners
     const long long col = ctile * WC_CW + cc;
     const bool col_ok = col < c.ncols;
-    const int xm = col_ok ? (int)((col / c.csmu) % c.Lmu) : 0;
+    const int csmu = w.csmu[pl], Lmu = w.Lmu[pl];
+    const int xm = col_ok ? (int)(((unsigned)col / (unsigned)csmu) % (unsigned)Lmu) : 0;
+    const CField<N, T> upl{up.p + (long long)pl * w.pstride, up.n};
+    double *accp = acc + (size_t)pl * w.npairs * WC_WARPS;
     long long colL = col;
     int xl = xm;
     Mat<N, T> S0, S1;  // S'_L at rows q and q + WC_PT of this column
     for (int L = 1; L <= w.lmax; ++L) {
       if (L > 1) {
-        if (++xl == c.Lmu) {
+        if (++xl == Lmu) {
           xl = 0;
-          colL -= (long long)(c.Lmu - 1) * c.csmu;
+          colL -= (long long)(Lmu - 1) * csmu;
         } else {
-          colL += c.csmu;
+          colL += csmu;
         }
       }
       T *sb = buf + (stage * WC_CW + cc) * CS;
@@ -664,10 +680,10 @@ __global__ void __launch_bounds__(WC_THREADS, WCMinBlocks<T>::v)
         // both rows' loads in flight before the first product
         const long long cbase = colL * c.rows + r0 + q;
         const bool two = q + WC_PT < rneed;
-        const Mat<N, T> u0 = up.load_t(cbase);
+        const Mat<N, T> u0 = upl.load_t(cbase);
         // FP32: the second row's load too (FP64 has no registers to spare for it)
         Mat<N, T> u1;
-        if constexpr (sizeof(T) == 4) u1 = two ? up.load_t(cbase + WC_PT) : mzero<N, T>();
+        if constexpr (sizeof(T) == 4) u1 = two ? upl.load_t(cbase + WC_PT) : mzero<N, T>();
         S0 = L == 1 ? u0 : mul(S0, u0);
 #pragma unroll
         for (int a = 0; a < N * N; ++a) {
@@ -675,7 +691,7 @@ __global__ void __launch_bounds__(WC_THREADS, WCMinBlocks<T>::v)
           sb[(2 * a + 1) * RS + q] = S0.e[a / N][a % N].im;
         }
         if (two) {
-          if constexpr (sizeof(T) == 8) u1 = up.load_t(cbase + WC_PT);
+          if constexpr (sizeof(T) == 8) u1 = upl.load_t(cbase + WC_PT);
           S1 = L == 1 ? u1 : mul(S1, u1);
 #pragma unroll
           for (int a = 0; a < N * N; ++a) {
@@ -707,13 +723,13 @@ __global__ void __launch_bounds__(WC_THREADS, WCMinBlocks<T>::v)
       const int j = (lane >> 2) & 7;
       if ((lane & 3) == 0) {
         const int p = w.pm[L][j];
-        if (p >= 0) acc[p * WC_WARPS + warp] += (double)tot;
+        if (p >= 0) accp[p * WC_WARPS + warp] += (double)tot;
       }
       stage ^= 1;
     }
   }
   __syncthreads();
-  for (int p = tid; p < w.npairs; p += WC_THREADS) {
+  for (int p = tid; p < nout; p += WC_THREADS) {
     double s = 0.0;
 #pragma unroll
     for (int q2 = 0; q2 < WC_WARPS; ++q2) s += acc[p * WC_WARPS + q2];
@@ -734,13 +750,14 @@ static bool wcorr_eligible(int tmax, const int *T, int nent) {
 }
 
 // Scratch needed by launch_wilson_gf (bytes).
-size_t wilson_gf_scratch(int nc, int dtype, const Geom &g, int nu, int tmax) {
+size_t wilson_gf_scratch(int nc, int dtype, const Geom &g, int nu, int tmax, int nplanes) {
   // bytes per site of a scratch field (CField: FP32 entries in 16-byte pairs)
   const size_t es = dtype == 0 ? 16 * (size_t)nc * nc : 16 * (size_t)((nc * nc + 1) / 2);
   const size_t rows = (size_t)g.L[nu] + (size_t)tmax;
   const size_t ncols = (size_t)(g.V / g.L[nu]);
   auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
-  return al(es * g.V) + al(es * ncols) + al(es * ncols * rows);
+  // Omega, P, and one U' per plane
+  return al(es * g.V) + al(es * ncols) + (size_t)nplanes * al(es * ncols * rows);
 }
 
 // R origin rows per column tile (even: each thread owns two), CW columns per CTA.
@@ -774,64 +791,80 @@ int wilson_gf_blocks(const Geom &g) {
   return sms * 4;
 }
 
+// The loops of nplanes planes (mus[i], nu) that share nu: one Omega, one U' per
+// plane, then the loop kernel; plane i's partial sums at d_part[(i * npairs + k) * grid + b].
 template <int N, typename T>
 static cudaError_t wilson_gf_t(const void *links, const Geom &g, const int *const *h_tab, int lmax, int tmax,
-                               int npairs, int mu, int nu, bool omega_ready, void *scratch, double *d_part, int nblk,
-                               int *grid_used, cudaStream_t st) {
+                               int npairs, const int *mus, int nplanes, int nu, bool omega_ready, void *scratch,
+                               double *d_part, int nblk, int *grid_used, cudaStream_t st) {
   auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+  if (nplanes < 1 || nplanes > WC_MAXPL) return cudaErrorInvalidValue;
+  if (npairs > WL_MAXP || lmax > WL_MAXP || tmax > 32767) return cudaErrorInvalidValue;
   const size_t es = CField<N, T>::bytes(1);
-  const ColGeom c = make_colgeom(g, mu, nu, g.L[nu] + tmax);
-  const long long Vc = c.ncols * g.L[nu];
+  ColGeom c[WC_MAXPL];
+  for (int i = 0; i < nplanes; ++i) c[i] = make_colgeom(g, mus[i], nu, g.L[nu] + tmax);
+  const long long Vc = c[0].ncols * g.L[nu];
+  const size_t up_bytes = al(es * c[0].ncols * c[0].rows);
   char *base = (char *)scratch;
   CField<N, T> om{(cx<T> *)base, Vc};
-  CField<N, T> pol{(cx<T> *)(base + al(es * Vc)), c.ncols};
-  CField<N, T> up{(cx<T> *)(base + al(es * Vc) + al(es * c.ncols)), c.ncols * c.rows};
+  CField<N, T> pol{(cx<T> *)(base + al(es * Vc)), c[0].ncols};
+  char *up0 = base + al(es * Vc) + al(es * c[0].ncols);
   Links<N, T> U{(cx<T> *)links, g.V};
-  if (!omega_ready) omega_kernel<N, T><<<(unsigned)((c.ncols + 127) / 128), 128, 0, st>>>(U, g, c, om, pol);
-  const long long nct = (c.ncols + 31) / 32;
-  uprime_kernel<N, T><<<(unsigned)(nct * ((c.rows + UP_RB - 1) / UP_RB)), 32 * UP_RB, 0, st>>>(U, g, c, om, pol,
-                                                                                             up);
-  if (npairs > WL_MAXP || lmax > WL_MAXP || tmax > 32767) return cudaErrorInvalidValue;
-  {
-    if (wcorr_eligible(tmax, h_tab[1], h_tab[0][lmax + 1])) {
-      WCTable w;
-      std::memset(&w, 0, sizeof w);
-      w.lmax = lmax;
-      w.npairs = npairs;
-      for (int L = 0; L <= WL_MAXP; ++L)
-        for (int j = 0; j < WC_TW; ++j) w.pm[L][j] = -1;
-      bool dup = false;
-      for (int L = 1; L <= lmax; ++L)
-        for (int k = h_tab[0][L]; k < h_tab[0][L + 1]; ++k) {
-          short &m = w.pm[L][h_tab[1][k] - 1];
-          dup = dup || m >= 0;
-          m = (short)h_tab[2][k];
-        }
-      if (!dup) {
-        w.R = g.L[nu] < WC_RO ? g.L[nu] : WC_RO;
-        w.ntile_rows = (g.L[nu] + w.R - 1) / w.R;
-        w.ntiles = ((c.ncols + WC_CW - 1) / WC_CW) * w.ntile_rows;
-        const size_t smem = wcorr_smem<N, T>(npairs);
-        // the attribute is per device: set it on every launch
-        cudaFuncSetAttribute(wcorr_kernel<N, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 112 * 1024);
-        // resident CTAs on the device, queried once per (N, T) (thread-safe static initialisation)
-        static const long long want = [] {
-          int dev = 0, sms = 0, nb = 0;
-          cudaGetDevice(&dev);
-          cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, wcorr_kernel<N, T>, WC_THREADS,
-                                                        wcorr_smem<N, T>(WL_MAXP));
-          return (long long)(sms > 0 ? sms : 148) * (nb > 0 ? nb : 1);
-        }();
-        const int grid = (int)std::min<long long>(std::min<long long>(want, nblk), w.ntiles > 0 ? w.ntiles : 1);
-        wcorr_kernel<N, T><<<grid, WC_THREADS, smem, st>>>(up, c, w, tmax, d_part);
-        cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess) return e;
-        *grid_used = grid;
-        return cudaSuccess;
+  if (!omega_ready) omega_kernel<N, T><<<(unsigned)((c[0].ncols + 127) / 128), 128, 0, st>>>(U, g, c[0], om, pol);
+  const long long nct = (c[0].ncols + 31) / 32;
+  for (int i = 0; i < nplanes; ++i) {
+    const CField<N, T> up{(cx<T> *)(up0 + i * up_bytes), c[i].ncols * c[i].rows};
+    uprime_kernel<N, T><<<(unsigned)(nct * ((c[i].rows + UP_RB - 1) / UP_RB)), 32 * UP_RB, 0, st>>>(U, g, c[i], om,
+                                                                                                 pol, up);
+  }
+  const CField<N, T> up{(cx<T> *)up0, c[0].ncols * c[0].rows};
+  if (wcorr_eligible(tmax, h_tab[1], h_tab[0][lmax + 1])) {
+    WCTable w;
+    std::memset(&w, 0, sizeof w);
+    w.lmax = lmax;
+    w.npairs = npairs;
+    for (int L = 0; L <= WL_MAXP; ++L)
+      for (int j = 0; j < WC_TW; ++j) w.pm[L][j] = -1;
+    bool dup = false;
+    for (int L = 1; L <= lmax; ++L)
+      for (int k = h_tab[0][L]; k < h_tab[0][L + 1]; ++k) {
+        short &m = w.pm[L][h_tab[1][k] - 1];
+        dup = dup || m >= 0;
+        m = (short)h_tab[2][k];
       }
+    if (!dup) {
+      w.R = g.L[nu] < WC_RO ? g.L[nu] : WC_RO;
+      w.ntile_rows = (g.L[nu] + w.R - 1) / w.R;
+      w.ntiles1 = ((c[0].ncols + WC_CW - 1) / WC_CW) * w.ntile_rows;
+      w.nplanes = nplanes;
+      w.pstride = (long long)(up_bytes / sizeof(cx<T>));
+      for (int i = 0; i < nplanes; ++i) {
+        w.mu[i] = mus[i];
+        w.csmu[i] = c[i].csmu;
+        w.Lmu[i] = c[i].Lmu;
+      }
+      const size_t smem = wcorr_smem<N, T>(npairs * nplanes);
+      // the attribute is per device: set it on every launch
+      cudaFuncSetAttribute(wcorr_kernel<N, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 120 * 1024);
+      // resident CTAs on the device, queried once per (N, T) (thread-safe static initialisation)
+      static const long long want = [] {
+        int dev = 0, sms = 0, nb = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, wcorr_kernel<N, T>, WC_THREADS,
+                                                      wcorr_smem<N, T>(WL_MAXP * WC_MAXPL));
+        return (long long)(sms > 0 ? sms : 148) * (nb > 0 ? nb : 1);
+      }();
+      const long long ntiles = w.ntiles1 * nplanes;
+      const int grid = (int)std::min<long long>(std::min<long long>(want, nblk), ntiles > 0 ? ntiles : 1);
+      wcorr_kernel<N, T><<<grid, WC_THREADS, smem, st>>>(up, c[0], w, tmax, d_part);
+      cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess) return e;
+      *grid_used = grid;
+      return cudaSuccess;
     }
   }
+  // entry-per-origin kernel: one launch per plane
   WLTable w;
   std::memset(&w, 0, sizeof w);
   w.lmax = lmax;
@@ -850,23 +883,27 @@ static cudaError_t wilson_gf_t(const void *links, const Geom &g, const int *cons
     }
   tile_shape(g, nu, w.R, w.CW);
   w.ntile_rows = (g.L[nu] + w.R - 1) / w.R;
-  w.ntiles = ((c.ncols + w.CW - 1) / w.CW) * w.ntile_rows;
+  w.ntiles = ((c[0].ncols + w.CW - 1) / w.CW) * w.ntile_rows;
   const size_t smem = (((size_t)npairs * WL_WARPS * sizeof(double) + 15) & ~(size_t)15) +
                       (size_t)TileEnt<N, T>::bytes * w.CW * (2 * ((w.R + tmax + 1) / 2));
   cudaFuncSetAttribute(wloop_kernel<N, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-  wloop_kernel<N, T><<<nblk, WL_THREADS, smem, st>>>(up, c, w, d_part);
+  for (int i = 0; i < nplanes; ++i) {
+    const CField<N, T> upi{(cx<T> *)(up0 + i * up_bytes), c[i].ncols * c[i].rows};
+    wloop_kernel<N, T><<<nblk, WL_THREADS, smem, st>>>(upi, c[i], w, d_part + (size_t)i * npairs * nblk);
+  }
   *grid_used = nblk;
   return cudaGetLastError();
 }
 
-cudaError_t launch_wilson_gf(int nc, int dtype, const void *links, const Geom &g, int mu, int nu,
-                             const int *const *h_tab, int lmax, int tmax, int npairs, bool omega_ready,
-                             void *scratch, double *d_part, int nblk, double *d_out, cudaStream_t st) {
+cudaError_t launch_wilson_gf(int nc, int dtype, const void *links, const Geom &g, const int *mus, int nplanes,
+                             int nu, const int *const *h_tab, int lmax, int tmax, int npairs, bool omega_ready,
+                             void *scratch, double *d_part, int nblk, double *d_out, int out_stride,
+                             cudaStream_t st) {
   cudaError_t e = cudaErrorInvalidValue;
   int grid = nblk;  // CTAs that wrote partial sums
-#define KLFT_WGF(NV, TV)                                                                                          \
-  e = wilson_gf_t<NV, TV>(links, g, h_tab, lmax, tmax, npairs, mu, nu, omega_ready, scratch, d_part, nblk, &grid, \
-                          st)
+#define KLFT_WGF(NV, TV)                                                                                        \
+  e = wilson_gf_t<NV, TV>(links, g, h_tab, lmax, tmax, npairs, mus, nplanes, nu, omega_ready, scratch, d_part, \
+                          nblk, &grid, st)
   if (dtype == 0) {
     if (nc == 1) KLFT_WGF(1, double);
     else if (nc == 2) KLFT_WGF(2, double);
@@ -878,7 +915,9 @@ cudaError_t launch_wilson_gf(int nc, int dtype, const void *links, const Geom &g
   }
 #undef KLFT_WGF
   if (e != cudaSuccess) return e;
-  return launch_reduce_partials(d_part, grid, npairs, d_out, st);
+  for (int i = 0; i < nplanes && e == cudaSuccess; ++i)
+    e = launch_reduce_partials(d_part + (size_t)i * npairs * grid, grid, npairs, d_out + (size_t)i * out_stride, st);
+  return e;
 }
 
 }  // namespace klft
