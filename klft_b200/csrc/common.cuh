@@ -118,9 +118,24 @@ template <int N, typename T> KLFT_HD Mat<N, T> mident() {
   for (int i = 0; i < N; ++i) m.e[i][i] = mk<T>(T(1), T(0));
   return m;
 }
+// SU(2) elements, and real combinations of them (staple sums, algebra
+// elements), have the form [[x, y], [-conj(y), conj(x)]]; so does every product
+// of two of them.  The products below form row 0 (in the general order) and
+// set row 1 from it: half the multiplications of the general 2x2 product.
+template <typename T> KLFT_HD void su2_row1(Mat<2, T> &c) {
+  c.e[1][0] = mk<T>(-c.e[0][1].re, c.e[0][1].im);
+  c.e[1][1] = mk<T>(c.e[0][0].re, -c.e[0][0].im);
+}
+
 // c = a * b (SUN.hpp:28-44 accumulation order)
 template <int N, typename T> KLFT_HD Mat<N, T> mul(const Mat<N, T> &a, const Mat<N, T> &b) {
   Mat<N, T> c;
+  if constexpr (N == 2) {
+    c.e[0][0] = a.e[0][0] * b.e[0][0] + a.e[0][1] * b.e[1][0];
+    c.e[0][1] = a.e[0][0] * b.e[0][1] + a.e[0][1] * b.e[1][1];
+    su2_row1(c);
+    return c;
+  }
 #pragma unroll
   for (int i = 0; i < N; ++i)
 #pragma unroll
@@ -135,6 +150,12 @@ template <int N, typename T> KLFT_HD Mat<N, T> mul(const Mat<N, T> &a, const Mat
 // c = a * b^dagger
 template <int N, typename T> KLFT_HD Mat<N, T> mul_nd(const Mat<N, T> &a, const Mat<N, T> &b) {
   Mat<N, T> c;
+  if constexpr (N == 2) {
+    c.e[0][0] = a.e[0][0] * conj(b.e[0][0]) + a.e[0][1] * conj(b.e[0][1]);
+    c.e[0][1] = a.e[0][0] * conj(b.e[1][0]) + a.e[0][1] * conj(b.e[1][1]);
+    su2_row1(c);
+    return c;
+  }
 #pragma unroll
   for (int i = 0; i < N; ++i)
 #pragma unroll
@@ -149,6 +170,12 @@ template <int N, typename T> KLFT_HD Mat<N, T> mul_nd(const Mat<N, T> &a, const 
 // c = a^dagger * b^dagger
 template <int N, typename T> KLFT_HD Mat<N, T> mul_dd(const Mat<N, T> &a, const Mat<N, T> &b) {
   Mat<N, T> c;
+  if constexpr (N == 2) {
+    c.e[0][0] = conj(a.e[0][0]) * conj(b.e[0][0]) + conj(a.e[1][0]) * conj(b.e[0][1]);
+    c.e[0][1] = conj(a.e[0][0]) * conj(b.e[1][0]) + conj(a.e[1][0]) * conj(b.e[1][1]);
+    su2_row1(c);
+    return c;
+  }
 #pragma unroll
   for (int i = 0; i < N; ++i)
 #pragma unroll
@@ -163,6 +190,12 @@ template <int N, typename T> KLFT_HD Mat<N, T> mul_dd(const Mat<N, T> &a, const 
 // c = a^dagger * b
 template <int N, typename T> KLFT_HD Mat<N, T> mul_dn(const Mat<N, T> &a, const Mat<N, T> &b) {
   Mat<N, T> c;
+  if constexpr (N == 2) {
+    c.e[0][0] = conj(a.e[0][0]) * b.e[0][0] + conj(a.e[1][0]) * b.e[1][0];
+    c.e[0][1] = conj(a.e[0][0]) * b.e[0][1] + conj(a.e[1][0]) * b.e[1][1];
+    su2_row1(c);
+    return c;
+  }
 #pragma unroll
   for (int i = 0; i < N; ++i)
 #pragma unroll
