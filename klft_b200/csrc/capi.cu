@@ -775,10 +775,14 @@ klft_status make_wilson_plan(klft_lattice *lat, const int *pairs, int npairs, in
     plan.off[plan.lmax + 1] = (int)plan.T.size();
     CK(lat->s_gf.ensure(wilson_gf_scratch(lat->nc, lat->dtype(), lat->g, nu, plan.tmax, nplanes)));
   }
-  CK(lat->s_tab.ensure((tab_off + h.size()) * sizeof(int) + 16));
-  CK(cudaMemcpyAsync((int *)lat->s_tab.ptr + tab_off, h.data(), h.size() * sizeof(int), cudaMemcpyHostToDevice,
-                     lat->stream));
-  CK(cudaStreamSynchronize(lat->stream));  // h is pageable and local
+  if (!plan.gf) {
+    // only the direct form reads the pairs on the device (the gauge-fixed form
+    // takes its tables in the kernel parameters): no copy, and no wait, otherwise
+    CK(lat->s_tab.ensure((tab_off + h.size()) * sizeof(int) + 16));
+    CK(cudaMemcpyAsync((int *)lat->s_tab.ptr + tab_off, h.data(), h.size() * sizeof(int), cudaMemcpyHostToDevice,
+                       lat->stream));
+    CK(cudaStreamSynchronize(lat->stream));  // h is pageable and local
+  }
   const int nblk = plan.gf ? wilson_gf_blocks(lat->g) : plaquette_blocks(lat->g);
   CK(lat->s_part.ensure((size_t)nblk * (npairs > 1 ? npairs : 1) * (size_t)nplanes * sizeof(double)));
   return KLFT_OK;
@@ -787,13 +791,13 @@ klft_status make_wilson_plan(klft_lattice *lat, const int *pairs, int npairs, in
 // enqueue: d_out[k] = unnormalised sum over sites of Re Tr W for pair k of the plan
 klft_status enqueue_wilson_plane(klft_lattice *lat, const WilsonPlan &plan, int mu, int nu, bool omega_ready,
                                  double *d_out) {
-  const int *tab = (const int *)lat->s_tab.ptr + plan.tab_off;
   if (plan.gf) {
     const int *ht[3] = {plan.off.data(), plan.T.data(), plan.p.data()};
     CK(launch_wilson_gf(lat->nc, lat->dtype(), lat->links, lat->g, &mu, 1, nu, ht, plan.lmax, plan.tmax,
                         plan.npairs, omega_ready, lat->s_gf.ptr, (double *)lat->s_part.ptr, wilson_gf_blocks(lat->g),
                         d_out, plan.npairs, lat->stream));
   } else {
+    const int *tab = (const int *)lat->s_tab.ptr + plan.tab_off;
     const int nblk = plaquette_blocks(lat->g);
     CK(launch_wilson_direct(lat->nc, lat->dtype(), lat->links, lat->g, mu, nu, tab, plan.npairs,
                             (double *)lat->s_part.ptr, nblk, d_out, lat->stream));
