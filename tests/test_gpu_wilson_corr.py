@@ -64,3 +64,16 @@ def test_tables_outside_the_correlation_form_agree(oracle):
     ref = oracle.wilson_temporal(lat, U, base + [(2, 9)])
     np.testing.assert_allclose(w_long, ref, rtol=0, atol=ATOL)
     g.close()
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_largest_pair_table_over_three_planes(oracle, precision):
+    """128 pairs (L up to 16, past the lattice) over the three spatial planes in
+    one launch: the largest per-CTA accumulator block (128 x 3 sums)."""
+    L = [6, 4, 4, 10]
+    lat, U, g = field(oracle, 3, L, 47, precision)
+    pairs = [(l, t) for l in range(1, 17) for t in range(1, 9)]
+    assert len(pairs) == 128
+    np.testing.assert_allclose(g.wilson_loop_temporal(pairs), oracle.wilson_temporal(lat, U, pairs),
+                               **TOL[precision])
+    g.close()
