@@ -21,8 +21,9 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::v)
   add_accepts(nacc, d_nacc);
 }
 
-// link pass val = 2 mu + p: U_mu(x) of the V/2 sites of parity p
-template <int ND, typename T, bool DF>
+// link pass val = 2 MU + p: U_MU(x) of the V/2 sites of parity p (one
+// instance per direction, so the staple's site steps are compiled)
+template <int ND, typename T, bool DF, int MU>
 __global__ void __launch_bounds__(128, MinBlocks<T>::v)
     metropolis_exp_kernel(Links<3, T> U, Geom g, int val, MetroArgs a, const uint32_t *__restrict__ d_sweep,
                           unsigned long long *__restrict__ d_nacc, Defect df) {
@@ -30,7 +31,7 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::v)
   int nacc = 0;
   bool ok = false;
   const Site x = link_pass_site(g, t, val & 1, ND, ok);
-  if (ok && t < link_pass_threads(g, ND)) nacc = link_update_exp<ND, T, DF>(U, g, x, val >> 1, a, *d_sweep, df);
+  if (ok && t < link_pass_threads(g, ND)) nacc = link_update_exp<ND, T, DF, MU>(U, g, x, MU, a, *d_sweep, df);
   add_accepts(nacc, d_nacc);
 }
 
@@ -42,7 +43,20 @@ static cudaError_t launch_tdf(const Links<NC, T> &U, const Geom &g, int val, con
   if constexpr (NC == 3) {
     if (a.proposal == PROPOSAL_EXP) {
       const unsigned lgrid = (unsigned)((link_pass_threads(g, ND) + block - 1) / block);
-      metropolis_exp_kernel<ND, T, DF><<<lgrid, block, 0, st>>>(U, g, val, a, d_sweep, d_nacc, df);
+      switch (val >> 1) {
+        case 0: metropolis_exp_kernel<ND, T, DF, 0><<<lgrid, block, 0, st>>>(U, g, val, a, d_sweep, d_nacc, df); break;
+        case 1: metropolis_exp_kernel<ND, T, DF, 1><<<lgrid, block, 0, st>>>(U, g, val, a, d_sweep, d_nacc, df); break;
+        case 2:
+          if constexpr (ND > 2)
+            metropolis_exp_kernel<ND, T, DF, (ND > 2 ? 2 : 0)><<<lgrid, block, 0, st>>>(U, g, val, a, d_sweep, d_nacc,
+                                                                                       df);
+          break;
+        default:
+          if constexpr (ND > 3)
+            metropolis_exp_kernel<ND, T, DF, (ND > 3 ? 3 : 0)><<<lgrid, block, 0, st>>>(U, g, val, a, d_sweep, d_nacc,
+                                                                                       df);
+          break;
+      }
       return cudaGetLastError();
     }
   }
