@@ -68,6 +68,72 @@ template <typename T> struct MinBlocks { static constexpr int v = 4; };
 template <> struct MinBlocks<double> { static constexpr int v = 2; };
 
 // Reference proposals: sequential per-site stream, exactly as the reference consumes it.
+// The hits of link U_mu(x) in the reference's order (Metropolis.hpp:85-107),
+// drawing from the site's stream rng.  MU >= 0: mu at compile time (the staple's
+// site steps compiled, its nu loops unrolled); MU = -1: run-time mu.
+template <int NC, int ND, typename T, bool DF, int MU>
+KLFT_D int link_update_ref(const Links<NC, T> &U, const Geom &g, const Site &x, int mu, const MetroArgs &a,
+                           const Defect &df, Stream &rng, long long lx, T bnc) {
+  if (open_link(g, x, mu)) return 0;
+  int nacc = 0;
+  Mat<NC, T> S;
+  if constexpr (MU >= 0) S = staple_ct<NC, ND, (MU >= 0 ? MU : 0), T>(U, g, x);
+  else S = staple<NC, ND, T, DF>(U, g, x, mu, df);
+  const bool dlink = DF && df.active && in_defect(g, df, x, mu);
+  if constexpr (NC <= 2) {
+    // U(1), SU(2): accepted proposals accumulate into A = r_1 ... r_k, so the
+    // current link is U0 A and Re Tr(U0 A r S) = Re Tr((A r) M0), M0 = S U0: one
+    // product A r per hit, which is also the new A on acceptance (warps take the
+    // accept branch on almost every hit).  The link is rebuilt as U0 A and
+    // reunitarised once; the chain is the one of U <- restore(U r) per accepted
+    // hit, with rounding-level differences.
+    const Mat<NC, T> U0 = U.load(lx, mu);
+    const Mat<NC, T> M0 = mul(S, U0);
+    Mat<NC, T> A = mident<NC, T>();
+    T trO = retr_diag(M0);
+    bool changed = false;
+#pragma unroll 1
+    for (int hit = 0; hit < a.nhits; ++hit) {
+      const Mat<NC, T> rr = propose<T>(rng, (const Mat<NC, T> *)nullptr, a.delta, PROPOSAL_REFERENCE, 0.0);
+      const Mat<NC, T> Y = hit == 0 ? rr : mul(A, rr);
+      const T tY = retr_mul(Y, M0);
+      T dS = -bnc * (tY - trO);
+      if (dlink) dS *= (T)defect_c(df);
+      bool accept = dS < T(0);
+      if (!accept) accept = rng.next() < (double)exp(-dS);
+      if (accept) {
+        A = Y;
+        trO = tY;
+        ++nacc;
+        changed = true;
+      }
+    }
+    if (changed) U.store(lx, mu, restore(mul(U0, A)));
+    return nacc;
+  }
+  Mat<NC, T> Uo = U.load(lx, mu);
+  Mat<NC, T> M = mul(S, Uo);
+  T trO = retr_diag(M);
+  bool changed = false;
+#pragma unroll 1
+  for (int hit = 0; hit < a.nhits; ++hit) {
+    const Mat<NC, T> rr = propose<T>(rng, (const Mat<NC, T> *)nullptr, a.delta, PROPOSAL_REFERENCE, 0.0);
+    T dS = -bnc * (retr_mul(rr, M) - trO);
+    if (dlink) dS *= (T)defect_c(df);
+    bool accept = dS < T(0);
+    if (!accept) accept = rng.next() < (double)exp(-dS);
+    if (accept) {
+      Uo = restore(mul(Uo, rr));
+      M = mul(S, Uo);
+      trO = retr_diag(M);
+      ++nacc;
+      changed = true;
+    }
+  }
+  if (changed) U.store(lx, mu, Uo);
+  return nacc;
+}
+
 template <int NC, int ND, typename T, bool DF>
 KLFT_D int site_update_ref(const Links<NC, T> &U, const Geom &g, const Site &x, const MetroArgs &a, uint32_t sweep,
                            const Defect &df) {
@@ -75,62 +141,15 @@ KLFT_D int site_update_ref(const Links<NC, T> &U, const Geom &g, const Site &x, 
   Stream rng(a.seed, a.chain, site_lex(g, x), sweep, KIND_METROPOLIS, 0);
   const long long lx = site_lin(g, x);
   const T bnc = (T)a.beta / (T)NC;
+  if constexpr (NC <= 2 && !DF) {
+    // U(1), SU(2): the directions unrolled, each with its compiled staple
+    nacc += link_update_ref<NC, ND, T, DF, 0>(U, g, x, 0, a, df, rng, lx, bnc);
+    nacc += link_update_ref<NC, ND, T, DF, 1>(U, g, x, 1, a, df, rng, lx, bnc);
+    if constexpr (ND > 2) nacc += link_update_ref<NC, ND, T, DF, (ND > 2 ? 2 : 0)>(U, g, x, 2, a, df, rng, lx, bnc);
+    if constexpr (ND > 3) nacc += link_update_ref<NC, ND, T, DF, (ND > 3 ? 3 : 0)>(U, g, x, 3, a, df, rng, lx, bnc);
+  } else {
 #pragma unroll 1
-  for (int mu = 0; mu < ND; ++mu) {
-    if (open_link(g, x, mu)) continue;
-    const Mat<NC, T> S = staple<NC, ND, T, DF>(U, g, x, mu, df);
-    const bool dlink = DF && df.active && in_defect(g, df, x, mu);
-    if constexpr (NC <= 2) {
-      // U(1), SU(2): accepted proposals accumulate into A = r_1 ... r_k, so the
-      // current link is U0 A and Re Tr(U0 A r S) = Re Tr((A r) M0), M0 = S U0: one
-      // product A r per hit, which is also the new A on acceptance (warps take the
-      // accept branch on almost every hit).  The link is rebuilt as U0 A and
-      // reunitarised once; the chain is the one of U <- restore(U r) per accepted
-      // hit, with rounding-level differences.
-      const Mat<NC, T> U0 = U.load(lx, mu);
-      const Mat<NC, T> M0 = mul(S, U0);
-      Mat<NC, T> A = mident<NC, T>();
-      T trO = retr_diag(M0);
-      bool changed = false;
-#pragma unroll 1
-      for (int hit = 0; hit < a.nhits; ++hit) {
-        const Mat<NC, T> rr = propose<T>(rng, (const Mat<NC, T> *)nullptr, a.delta, PROPOSAL_REFERENCE, 0.0);
-        const Mat<NC, T> Y = hit == 0 ? rr : mul(A, rr);
-        const T tY = retr_mul(Y, M0);
-        T dS = -bnc * (tY - trO);
-        if (dlink) dS *= (T)defect_c(df);
-        bool accept = dS < T(0);
-        if (!accept) accept = rng.next() < (double)exp(-dS);
-        if (accept) {
-          A = Y;
-          trO = tY;
-          ++nacc;
-          changed = true;
-        }
-      }
-      if (changed) U.store(lx, mu, restore(mul(U0, A)));
-      continue;
-    }
-    Mat<NC, T> Uo = U.load(lx, mu);
-    Mat<NC, T> M = mul(S, Uo);
-    T trO = retr_diag(M);
-    bool changed = false;
-#pragma unroll 1
-    for (int hit = 0; hit < a.nhits; ++hit) {
-      const Mat<NC, T> rr = propose<T>(rng, (const Mat<NC, T> *)nullptr, a.delta, PROPOSAL_REFERENCE, 0.0);
-      T dS = -bnc * (retr_mul(rr, M) - trO);
-      if (dlink) dS *= (T)defect_c(df);
-      bool accept = dS < T(0);
-      if (!accept) accept = rng.next() < (double)exp(-dS);
-      if (accept) {
-        Uo = restore(mul(Uo, rr));
-        M = mul(S, Uo);
-        trO = retr_diag(M);
-        ++nacc;
-        changed = true;
-      }
-    }
-    if (changed) U.store(lx, mu, Uo);
+    for (int mu = 0; mu < ND; ++mu) nacc += link_update_ref<NC, ND, T, DF, -1>(U, g, x, mu, a, df, rng, lx, bnc);
   }
   return nacc;
 }
@@ -219,7 +238,7 @@ KLFT_D int link_update_exp(const Links<3, T> &U, const Geom &g, const Site &x, i
   Mat<3, T> S;
   constexpr int MC = MU >= 0 ? MU : 0;
   if constexpr (MU >= 0 && !DF && sizeof(T) == 4) S = staple_su3_2row_ct<ND, MC>(U, g, x);
-  else if constexpr (MU >= 0 && !DF) S = staple_ct<3, ND, MC, T>(U, g, x);
+  else if constexpr (MU >= 0) S = staple_ct<3, ND, MC, T, DF>(U, g, x, df);
   else if constexpr (sizeof(T) == 4 && !DF) S = staple_su3_2row<ND>(U, g, x, mu);
   else S = staple<3, ND, T, DF>(U, g, x, mu, df);
   const Mat<3, T> M0 = mul(U.load(lx, mu), S);
