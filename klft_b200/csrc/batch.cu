@@ -60,7 +60,8 @@ KLFT_D int find_chain(const ChainTable &tab) {
   return lo;
 }
 
-template <int NC, int ND, typename T, bool EXP, bool DF>
+// MU >= 0 (exp groups): the link pass's direction at compile time (val >> 1 == MU)
+template <int NC, int ND, typename T, bool EXP, bool DF, int MU = -1>
 __global__ void __launch_bounds__(128, MinBlocks<T>::v)
     multi_pass_kernel(const __grid_constant__ ChainTable tab, int val, unsigned long long *nacc_slots,
                       const uint32_t *__restrict__ slot) {
@@ -72,7 +73,8 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::v)
   if constexpr (EXP && NC == 3) {
     bool ok = false;
     const Site x = link_pass_site(c.g, t, val & 1, ND, ok);
-    if (ok && t < link_pass_threads(c.g, ND)) nacc = link_update_exp<ND, T, DF>(U, c.g, x, val >> 1, c.a, *c.ctr, c.df);
+    if (ok && t < link_pass_threads(c.g, ND))
+      nacc = link_update_exp<ND, T, DF, MU>(U, c.g, x, MU >= 0 ? MU : val >> 1, c.a, *c.ctr, c.df);
   } else {
     if (t < c.g.Vh) nacc = site_update_ref<NC, ND, T, DF>(U, c.g, pass_site(c.g, t, val, ND), c.a, *c.ctr, c.df);
   }
@@ -296,7 +298,23 @@ struct GroupKey {
 template <int NC, int ND, typename T, bool EXP, bool DF>
 cudaError_t launch_group_t(const ChainTable &tab, int blocks, int val, unsigned long long *nacc, const uint32_t *slot,
                            cudaStream_t st) {
-  multi_pass_kernel<NC, ND, T, EXP, DF><<<blocks, tab.block, 0, st>>>(tab, val, nacc, slot);
+  if constexpr (EXP && NC == 3) {
+    // one kernel instance per link direction (compiled staple site steps)
+    switch (val >> 1) {
+      case 0: multi_pass_kernel<NC, ND, T, EXP, DF, 0><<<blocks, tab.block, 0, st>>>(tab, val, nacc, slot); break;
+      case 1: multi_pass_kernel<NC, ND, T, EXP, DF, 1><<<blocks, tab.block, 0, st>>>(tab, val, nacc, slot); break;
+      case 2:
+        if constexpr (ND > 2)
+          multi_pass_kernel<NC, ND, T, EXP, DF, (ND > 2 ? 2 : 0)><<<blocks, tab.block, 0, st>>>(tab, val, nacc, slot);
+        break;
+      default:
+        if constexpr (ND > 3)
+          multi_pass_kernel<NC, ND, T, EXP, DF, (ND > 3 ? 3 : 0)><<<blocks, tab.block, 0, st>>>(tab, val, nacc, slot);
+        break;
+    }
+  } else {
+    multi_pass_kernel<NC, ND, T, EXP, DF><<<blocks, tab.block, 0, st>>>(tab, val, nacc, slot);
+  }
   return cudaGetLastError();
 }
 

@@ -147,24 +147,27 @@ KLFT_D Mat<3, float> staple_su3_2row_ct(const Links<3, float> &U, const Geom &g,
 // same products in the same order, but every site step and index folds to a few
 // integer operations.  For kernels without proposal code (the HMC force), where
 // the unrolled products fit the instruction cache.
-template <int NC, int ND, int MU, typename T>
-KLFT_D Mat<NC, T> staple_ct(const Links<NC, T> &U, const Geom &g, const Site &x) {
+// DF: the PTBC defect factors as in staple() (only links of direction 0 can
+// carry one, which the compiled direction makes visible to the compiler).
+template <int NC, int ND, int MU, typename T, bool DF = false>
+KLFT_D Mat<NC, T> staple_ct(const Links<NC, T> &U, const Geom &g, const Site &x, const Defect &df = Defect{}) {
   Mat<NC, T> S = mzero<NC, T>();
   const Site xpmu = site_up(g, x, MU);
 #pragma unroll
   for (int nu = 0; nu < ND; ++nu) {
     if (nu == MU) continue;
     const Site xpnu = site_up(g, x, nu);
-    const Mat<NC, T> t = mul_nd(U.load(site_lin(g, xpmu), nu), U.load(site_lin(g, xpnu), MU));
-    madd(S, mul_nd(t, U.load(site_lin(g, x), nu)));
+    const Mat<NC, T> t = mul_nd(load_link<NC, T, DF>(U, g, xpmu, nu, df), load_link<NC, T, DF>(U, g, xpnu, MU, df));
+    madd(S, mul_nd(t, load_link<NC, T, DF>(U, g, x, nu, df)));
   }
 #pragma unroll
   for (int nu = 0; nu < ND; ++nu) {
     if (nu == MU) continue;
     const Site xpmu_mnu = site_dn(g, xpmu, nu);
     const Site xmnu = site_dn(g, x, nu);
-    const Mat<NC, T> t = mul_dd(U.load(site_lin(g, xpmu_mnu), nu), U.load(site_lin(g, xmnu), MU));
-    madd(S, mul(t, U.load(site_lin(g, xmnu), nu)));
+    const Mat<NC, T> t =
+        mul_dd(load_link<NC, T, DF>(U, g, xpmu_mnu, nu, df), load_link<NC, T, DF>(U, g, xmnu, MU, df));
+    madd(S, mul(t, load_link<NC, T, DF>(U, g, xmnu, nu, df)));
   }
   return S;
 }
