@@ -312,7 +312,7 @@ def cpu_baseline_reference(L: int):
 
 # DRAM traffic of one link pass (dram__bytes_read.sum + dram__bytes_write.sum of one
 # metropolis_exp_kernel launch in the ncu capture summarised in the profile below).
-TRAFFIC_PASS_BYTES = 204574976 + 18085888
+TRAFFIC_PASS_BYTES = 204658944 + 19519744
 TRAFFIC_SOURCE = "profiles/metropolis_exp_su3_32x4_mixed.md"
 
 
