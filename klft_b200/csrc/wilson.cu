@@ -14,9 +14,10 @@
 // Per (site, L, T) the loop costs one trace of a product (18 FMAs for SU(3))
 // instead of the ~4 matrix products of the direct form.
 //
-// Kernels: omega_kernel (per nu: the axial-gauge transformation, FP64),
-// uprime_kernel (per plane: U'_mu on L_nu + T_max rows, computed in FP64 and
-// stored in the link precision), wloop_kernel (per plane: persistent CTAs over
+// Kernels: omega_kernel (per nu: the axial-gauge transformation, products in
+// FP64, stored in the link precision), uprime_kernel (per plane: U'_mu on
+// L_nu + T_max rows in the link precision), wcorr_kernel (the column-correlation
+// form below, all planes of one nu in one launch), wloop_kernel (per plane: persistent CTAs over
 // tiles of CW columns x R rows; S'_L is built incrementally over L in shared
 // memory together with a halo of T_max rows of the same column; per-site traces
 // in the link precision, lattice sums in FP64).
