@@ -41,6 +41,7 @@ L_DEFAULT = 32
 BETA, NHITS = 6.0, 10
 PAIRS = [(l, t) for l in range(1, 9) for t in range(1, 9)]
 METRIC = "Link updates/s (SU(3) 32^4), mixed vs FP64 form; serving p50/p99 job latency"
+REF_WARMUP_S, REF_TIMED_S = 30.0, 120.0  # time bounds of the reference arm (host cycles of seconds each)
 
 
 def parse():
@@ -768,20 +769,30 @@ def run_reference(a, dist: Dist):
     U = lat.field()
     for c in range(3):
         U[:, :, c, c] = 1.0
-    for k in range(a.warmup):
-        r.cycles(lat, U, BETA, 0.1, NHITS, 1, 1234, PAIRS, sweep0=k)
+    # A step is one whole cycle (seconds on the host), so the run is bounded by
+    # time: at most REF_WARMUP_S of warm-up cycles (at least one) and the timed
+    # cycles stop once REF_TIMED_S have passed (at least one is timed).
+    nwarm = 0
+    tw = time.perf_counter()
+    while nwarm < max(1, a.warmup) and (nwarm == 0 or time.perf_counter() - tw < REF_WARMUP_S):
+        r.cycles(lat, U, BETA, 0.1, NHITS, 1, 1234, PAIRS, sweep0=nwarm)
+        nwarm += 1
     t0 = time.perf_counter()
-    for k in range(a.steps):
-        r.cycles(lat, U, BETA, 0.1, NHITS, 1, 1234, PAIRS, sweep0=a.warmup + k)
+    steps = 0
+    while steps < a.steps and (steps == 0 or time.perf_counter() - t0 < REF_TIMED_S):
+        r.cycles(lat, U, BETA, 0.1, NHITS, 1, 1234, PAIRS, sweep0=nwarm + steps)
+        steps += 1
     dt = time.perf_counter() - t0
-    v = lat.V * 4 * a.steps / dt
-    return {"metric": METRIC, "value": v, "unit": "link updates/s", "n_gpus": dist.world, "steps": a.steps,
-            "warmup": a.warmup, "ms_per_step": dt * 1e3 / a.steps, "higher_is_better": True, "scaling": "weak",
+    v = lat.V * 4 * steps / dt
+    return {"metric": METRIC, "value": v, "unit": "link updates/s", "n_gpus": dist.world, "steps": steps,
+            "steps_requested": a.steps, "warmup": nwarm, "warmup_requested": a.warmup,
+            "ms_per_step": dt * 1e3 / steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (cold start)", "impl": "reference",
             "config": {"workload": f"SU(3) 4D {a.L}^4 Metropolis beta=6 nHits=10 (reference SU(3) proposal), per "
                                    f"step 1 sweep + plaquette + W_temp(L,T in 1..8)", "parallelism": "host OpenMP"},
             "cpu_baseline": {"value": v, "unit": "link updates/s", "cores": cores, "kind": "reference",
-                             "sample": f"{a.steps} full cycles of SU(3) {a.L}^4 on {cores} host threads"},
+                             "sample": f"{steps} full cycles of SU(3) {a.L}^4 on {cores} host threads (time-bounded: "
+                                       f"{REF_WARMUP_S:.0f} s of warm-up, {REF_TIMED_S:.0f} s timed at most)"},
             "e2e": {"value": v, "unit": "link updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
