@@ -217,8 +217,10 @@ def e2e_public_api(g, eps, steps, per_call=False):
         h2d = pairs.nbytes * 3  # the pair list goes up once per spatial direction
         d2h = 8 + 8 + 8 * len(PAIRS) * 3
     else:
+        # up: the pair list (kernel parameters); down: one copy of the step's
+        # accept count, plaquette sum and the loop sums of the 3 spatial planes
         h2d = pairs.nbytes
-        d2h = 8 + 8 + 8 * len(PAIRS)
+        d2h = 8 + 8 + 8 * len(PAIRS) * 3
     return dt, h2d, d2h
 
 

@@ -478,11 +478,12 @@ klft_status klft_run_cycles(klft_lattice *lat, double beta, double delta, int nh
   LOCK(lat);
   const int nd = lat->g.nd;
   const int nw = (nd - 1) * npairs;  // per cycle: one sum per (spatial mu, pair)
-  // aux: nacc (ncycles u64); wl: [plaq ncycles][w ncycles*nw]; all scratch sized before the first launch
-  CK(lat->s_aux.ensure((size_t)ncycles * sizeof(unsigned long long)));
-  CK(lat->s_wl.ensure((size_t)ncycles * (1 + nw) * sizeof(double)));
-  unsigned long long *d_nacc = (unsigned long long *)lat->s_aux.ptr;
-  double *d_plaq = (double *)lat->s_wl.ptr;
+  // wl: [nacc ncycles (u64)][plaq ncycles][w ncycles*nw], one block so that one
+  // copy brings the results back; all scratch sized before the first launch
+  const size_t nres = (size_t)ncycles * (2 + nw);  // 8-byte slots
+  CK(lat->s_wl.ensure(nres * sizeof(double)));
+  unsigned long long *d_nacc = (unsigned long long *)lat->s_wl.ptr;
+  double *d_plaq = (double *)lat->s_wl.ptr + ncycles;
   double *d_w = d_plaq + ncycles;
   WilsonPlan plan;
   if (npairs > 0) {
@@ -520,12 +521,17 @@ klft_status klft_run_cycles(klft_lattice *lat, double beta, double delta, int nh
     }
   }
   CK(cudaEventRecord(e1, lat->stream));
-  std::vector<unsigned long long> h_nacc(ncycles);
-  std::vector<double> h_out((size_t)ncycles * (1 + nw));
-  CK(cudaMemcpyAsync(h_nacc.data(), d_nacc, (size_t)ncycles * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
-                     lat->stream));
-  CK(cudaMemcpyAsync(h_out.data(), d_plaq, h_out.size() * sizeof(double), cudaMemcpyDeviceToHost, lat->stream));
+  // into the handle's page-locked slots when the results fit (one DMA copy)
+  std::vector<double> h_big;
+  double *h_res = lat->h_results;
+  if (nres > KLFT_RESULT_SLOTS) {
+    h_big.resize(nres);
+    h_res = h_big.data();
+  }
+  CK(cudaMemcpyAsync(h_res, lat->s_wl.ptr, nres * sizeof(double), cudaMemcpyDeviceToHost, lat->stream));
   CK(cudaStreamSynchronize(lat->stream));
+  const unsigned long long *h_nacc = (const unsigned long long *)h_res;
+  const double *h_out = h_res + ncycles;
   float ms = 0.f;
   CK(cudaEventElapsedTime(&ms, e0, e1));
   cudaEventDestroy(e0);
