@@ -244,6 +244,12 @@ klft_status klft_lattice_destroy(klft_lattice *lat) {
     if (lat->links) cudaFreeAsync(lat->links, lat->stream);
     if (lat->d_counters) cudaFreeAsync(lat->d_counters, lat->stream);
     pinned_slots_put(lat->h_results);
+    if (lat->side) {
+      cudaStreamSynchronize(lat->side);
+      cudaStreamDestroy(lat->side);
+    }
+    if (lat->ev_fork) cudaEventDestroy(lat->ev_fork);
+    if (lat->ev_join) cudaEventDestroy(lat->ev_join);
     if (lat->stream) cudaStreamDestroy(lat->stream);
   }
   delete lat;
@@ -479,22 +485,31 @@ klft_status klft_run_cycles(klft_lattice *lat, double beta, double delta, int nh
   const int nd = lat->g.nd;
   const int nw = (nd - 1) * npairs;  // per cycle: one sum per (spatial mu, pair)
   // wl: [nacc ncycles (u64)][plaq ncycles][w ncycles*nw], one block so that one
-  // copy brings the results back; all scratch sized before the first launch
+  // copy brings the results back, then the plaquette's block partials (the loop
+  // kernels, which may run at the same time, keep theirs in s_part); all
+  // scratch sized before the first launch
   const size_t nres = (size_t)ncycles * (2 + nw);  // 8-byte slots
-  CK(lat->s_wl.ensure(nres * sizeof(double)));
+  const int nblk_plaq = plaquette_blocks(lat->g);
+  CK(lat->s_wl.ensure((nres + (size_t)nblk_plaq) * sizeof(double)));
   unsigned long long *d_nacc = (unsigned long long *)lat->s_wl.ptr;
   double *d_plaq = (double *)lat->s_wl.ptr + ncycles;
   double *d_w = d_plaq + ncycles;
+  double *d_plaq_part = (double *)lat->s_wl.ptr + nres;
+  // with loops to measure, the plaquette (which reads every link) runs on the
+  // side stream beside the loops' axial-gauge transformation (one thread per
+  // column: a latency-bound kernel that leaves most of the device idle)
+  const bool fork = measure_plaquette && npairs > 0;
+  if (fork && !lat->side) {
+    CK(cudaStreamCreateWithFlags(&lat->side, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&lat->ev_fork, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&lat->ev_join, cudaEventDisableTiming));
+  }
   WilsonPlan plan;
   if (npairs > 0) {
     klft_status s = make_wilson_plan(lat, temporal_pairs, npairs, nd - 1, plan, 0, nd - 1);
     if (s != KLFT_OK) return s;
   }
   CK(cudaMemsetAsync(d_nacc, 0, (size_t)ncycles * sizeof(unsigned long long), lat->stream));
-  {
-    const int nblk = plaquette_blocks(lat->g);
-    if (lat->s_part.cap < (size_t)nblk * sizeof(double)) CK(lat->s_part.ensure((size_t)nblk * sizeof(double)));
-  }
   // The temporal (1, 1) loop of plane (mu, Nd-1) is that plane's plaquette: when
   // the pair list holds it, the plaquette kernel covers the spatial planes only
   // and the temporal planes come from the loop sums (added in FP64 below).
@@ -509,16 +524,24 @@ klft_status klft_run_cycles(klft_lattice *lat, double beta, double delta, int nh
   for (int c = 0; c < ncycles; ++c) {
     klft_status s = enqueue_sweeps(lat, beta, delta, nhits, proposal, eps, 1, d_nacc + c, lat->defect);
     if (s != KLFT_OK) return s;
-    if (measure_plaquette) {
-      const int nblk = plaquette_blocks(lat->g);
-      CK(launch_plaquette(lat->nc, lat->dtype(), lat->links, lat->g, (double *)lat->s_part.ptr, nblk, d_plaq + c,
-                          lat->stream, plaq_nu_end));
+    if (fork) {
+      CK(cudaEventRecord(lat->ev_fork, lat->stream));
+      CK(cudaStreamWaitEvent(lat->side, lat->ev_fork, 0));
     }
+    if (measure_plaquette)
+      CK(launch_plaquette(lat->nc, lat->dtype(), lat->links, lat->g, d_plaq_part, nblk_plaq, d_plaq + c,
+                          fork ? lat->side : lat->stream, plaq_nu_end));
+    if (fork) CK(cudaEventRecord(lat->ev_join, lat->side));
     if (npairs > 0) {
       // the spatial planes share the axial-gauge transformation along nu = Nd-1
       s = enqueue_wilson_spatial(lat, plan, false, d_w + (size_t)c * nw, npairs);
-      if (s != KLFT_OK) return s;
+      if (s != KLFT_OK) {
+        if (fork) cudaStreamWaitEvent(lat->stream, lat->ev_join, 0);
+        return s;
+      }
     }
+    // the next sweep (and the result copy) after the plaquette
+    if (fork) CK(cudaStreamWaitEvent(lat->stream, lat->ev_join, 0));
   }
   CK(cudaEventRecord(e1, lat->stream));
   // into the handle's page-locked slots when the results fit (one DMA copy)

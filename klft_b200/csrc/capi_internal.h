@@ -64,6 +64,10 @@ struct klft_lattice {
   void *links = nullptr;
   size_t link_bytes = 0;
   cudaStream_t stream = nullptr;
+  // klft_run_cycles: a second stream for the plaquette beside the loops' axial
+  // gauge transformation (created on first use), with its fork / join events
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   uint32_t *d_counters = nullptr;  // [0] sweep, [1] trajectory, [2] cycle
   double *h_results = nullptr;     // pinned, KLFT_RESULT_SLOTS doubles
   klft::Scratch s_part, s_out, s_aux, s_stage, s_wl, s_hmc, s_gf, s_tab, s_tune;
