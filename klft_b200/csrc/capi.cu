@@ -248,8 +248,8 @@ klft_status klft_lattice_destroy(klft_lattice *lat) {
       cudaStreamSynchronize(lat->side);
       cudaStreamDestroy(lat->side);
     }
-    if (lat->ev_fork) cudaEventDestroy(lat->ev_fork);
-    if (lat->ev_join) cudaEventDestroy(lat->ev_join);
+    for (cudaEvent_t ev : {lat->ev_fork, lat->ev_join, lat->ev_up, lat->ev_loops})
+      if (ev) cudaEventDestroy(ev);
     if (lat->stream) cudaStreamDestroy(lat->stream);
   }
   delete lat;
@@ -495,20 +495,29 @@ klft_status klft_run_cycles(klft_lattice *lat, double beta, double delta, int nh
   double *d_plaq = (double *)lat->s_wl.ptr + ncycles;
   double *d_w = d_plaq + ncycles;
   double *d_plaq_part = (double *)lat->s_wl.ptr + nres;
-  // with loops to measure, the plaquette (which reads every link) runs on the
-  // side stream beside the loops' axial-gauge transformation (one thread per
-  // column: a latency-bound kernel that leaves most of the device idle)
-  const bool fork = measure_plaquette && npairs > 0;
-  if (fork && !lat->side) {
-    CK(cudaStreamCreateWithFlags(&lat->side, cudaStreamNonBlocking));
-    CK(cudaEventCreateWithFlags(&lat->ev_fork, cudaEventDisableTiming));
-    CK(cudaEventCreateWithFlags(&lat->ev_join, cudaEventDisableTiming));
-  }
   WilsonPlan plan;
   if (npairs > 0) {
     klft_status s = make_wilson_plan(lat, temporal_pairs, npairs, nd - 1, plan, 0, nd - 1);
     if (s != KLFT_OK) return s;
   }
+  // With loops to measure, two parts of a cycle run on the side stream: the
+  // plaquette (it reads every link) beside the loops' axial-gauge
+  // transformation (one thread per column: a latency-bound kernel that leaves
+  // most of the device idle), and the gauge-fixed form's loop kernels, which
+  // read only U', beside the next cycle's sweep.  Events order the rest: the
+  // next sweep waits for the plaquette, the next U' for the loops.
+  const bool fork = measure_plaquette && npairs > 0;
+  const bool loops_side = npairs > 0 && plan.gf;
+  if ((fork || loops_side) && !lat->side) {
+    CK(cudaStreamCreateWithFlags(&lat->side, cudaStreamNonBlocking));
+    for (cudaEvent_t *ev : {&lat->ev_fork, &lat->ev_join, &lat->ev_up, &lat->ev_loops})
+      CK(cudaEventCreateWithFlags(ev, cudaEventDisableTiming));
+  }
+  // on an early return: the main stream after everything enqueued on the side stream
+  auto join_side = [&] {
+    if ((fork || loops_side) && cudaEventRecord(lat->ev_join, lat->side) == cudaSuccess)
+      cudaStreamWaitEvent(lat->stream, lat->ev_join, 0);
+  };
   CK(cudaMemsetAsync(d_nacc, 0, (size_t)ncycles * sizeof(unsigned long long), lat->stream));
   // The temporal (1, 1) loop of plane (mu, Nd-1) is that plane's plaquette: when
   // the pair list holds it, the plaquette kernel covers the spatial planes only
@@ -523,26 +532,33 @@ klft_status klft_run_cycles(klft_lattice *lat, double beta, double delta, int nh
   CK(cudaEventRecord(e0, lat->stream));
   for (int c = 0; c < ncycles; ++c) {
     klft_status s = enqueue_sweeps(lat, beta, delta, nhits, proposal, eps, 1, d_nacc + c, lat->defect);
-    if (s != KLFT_OK) return s;
-    if (fork) {
-      CK(cudaEventRecord(lat->ev_fork, lat->stream));
-      CK(cudaStreamWaitEvent(lat->side, lat->ev_fork, 0));
+    cudaError_t e = cudaSuccess;
+    if (s == KLFT_OK && fork) {
+      e = cudaEventRecord(lat->ev_fork, lat->stream);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(lat->side, lat->ev_fork, 0);
     }
-    if (measure_plaquette)
-      CK(launch_plaquette(lat->nc, lat->dtype(), lat->links, lat->g, d_plaq_part, nblk_plaq, d_plaq + c,
-                          fork ? lat->side : lat->stream, plaq_nu_end));
-    if (fork) CK(cudaEventRecord(lat->ev_join, lat->side));
-    if (npairs > 0) {
+    if (s == KLFT_OK && e == cudaSuccess && measure_plaquette)
+      e = launch_plaquette(lat->nc, lat->dtype(), lat->links, lat->g, d_plaq_part, nblk_plaq, d_plaq + c,
+                           fork ? lat->side : lat->stream, plaq_nu_end);
+    if (s == KLFT_OK && e == cudaSuccess && fork) e = cudaEventRecord(lat->ev_join, lat->side);
+    // U' of this cycle after the loops of the previous one
+    if (s == KLFT_OK && e == cudaSuccess && loops_side && c > 0)
+      e = cudaStreamWaitEvent(lat->stream, lat->ev_loops, 0);
+    if (s == KLFT_OK && e == cudaSuccess && npairs > 0) {
       // the spatial planes share the axial-gauge transformation along nu = Nd-1
-      s = enqueue_wilson_spatial(lat, plan, false, d_w + (size_t)c * nw, npairs);
-      if (s != KLFT_OK) {
-        if (fork) cudaStreamWaitEvent(lat->stream, lat->ev_join, 0);
-        return s;
-      }
+      s = enqueue_wilson_spatial(lat, plan, false, d_w + (size_t)c * nw, npairs, loops_side ? lat->side : nullptr,
+                                 lat->ev_up);
+      if (s == KLFT_OK && loops_side) e = cudaEventRecord(lat->ev_loops, lat->side);
     }
-    // the next sweep (and the result copy) after the plaquette
-    if (fork) CK(cudaStreamWaitEvent(lat->stream, lat->ev_join, 0));
+    // the next sweep after the plaquette
+    if (s == KLFT_OK && e == cudaSuccess && fork) e = cudaStreamWaitEvent(lat->stream, lat->ev_join, 0);
+    if (s != KLFT_OK || e != cudaSuccess) {
+      join_side();
+      return s != KLFT_OK ? s : cuda_fail(e, "klft_run_cycles");
+    }
   }
+  // the result copy after the last loops
+  if (loops_side) CK(cudaStreamWaitEvent(lat->stream, lat->ev_loops, 0));
   CK(cudaEventRecord(e1, lat->stream));
   // into the handle's page-locked slots when the results fit (one DMA copy)
   std::vector<double> h_big;
@@ -839,7 +855,7 @@ klft_status enqueue_wilson_plane(klft_lattice *lat, const WilsonPlan &plan, int 
 // runs all planes in one loop-kernel launch (one tile queue, so the last wave of
 // one plane does not idle while the next plane waits for its own launch).
 klft_status enqueue_wilson_spatial(klft_lattice *lat, const WilsonPlan &plan, bool omega_ready, double *d_out,
-                                   int out_stride) {
+                                   int out_stride, cudaStream_t side, cudaEvent_t ev) {
   const int nu = lat->g.nd - 1;
   if (plan.gf) {
     const int *ht[3] = {plan.off.data(), plan.T.data(), plan.p.data()};
@@ -847,7 +863,7 @@ klft_status enqueue_wilson_spatial(klft_lattice *lat, const WilsonPlan &plan, bo
     // planes mu = 0 .. nu - 1
     CK(launch_wilson_gf(lat->nc, lat->dtype(), lat->links, lat->g, mus, nu, nu, ht, plan.lmax, plan.tmax,
                         plan.npairs, omega_ready, lat->s_gf.ptr, (double *)lat->s_part.ptr, wilson_gf_blocks(lat->g),
-                        d_out, out_stride, lat->stream));
+                        d_out, out_stride, lat->stream, side, ev));
     return KLFT_OK;
   }
   for (int mu = 0; mu < nu; ++mu) {

@@ -64,10 +64,12 @@ struct klft_lattice {
   void *links = nullptr;
   size_t link_bytes = 0;
   cudaStream_t stream = nullptr;
-  // klft_run_cycles: a second stream for the plaquette beside the loops' axial
-  // gauge transformation (created on first use), with its fork / join events
+  // klft_run_cycles: a second stream (created on first use) for the plaquette,
+  // beside the loops' axial-gauge transformation, and for the loop kernels,
+  // beside the next sweep; events: after the sweep, after the plaquette, after
+  // U', after the loops
   cudaStream_t side = nullptr;
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_up = nullptr, ev_loops = nullptr;
   uint32_t *d_counters = nullptr;  // [0] sweep, [1] trajectory, [2] cycle
   double *h_results = nullptr;     // pinned, KLFT_RESULT_SLOTS doubles
   klft::Scratch s_part, s_out, s_aux, s_stage, s_wl, s_hmc, s_gf, s_tab, s_tune;
@@ -137,7 +139,8 @@ klft_status make_wilson_plan(klft_lattice *lat, const int *pairs, int npairs, in
                              size_t tab_off = 0, int nplanes = 1);
 klft_status enqueue_wilson_plane(klft_lattice *lat, const WilsonPlan &plan, int mu, int nu, bool omega_ready,
                                  double *d_out);
+// side / ev: the gauge-fixed form's loop kernels on side after ev (see launch_wilson_gf)
 klft_status enqueue_wilson_spatial(klft_lattice *lat, const WilsonPlan &plan, bool omega_ready, double *d_out,
-                                   int out_stride);
+                                   int out_stride, cudaStream_t side = nullptr, cudaEvent_t ev = nullptr);
 klft_status wilson_sums(klft_lattice *lat, int mu, int nu, const int *pairs, int npairs, double *sums);
 }  // namespace klft

@@ -65,11 +65,13 @@ int wilson_gf_blocks(const Geom &g);
 constexpr int WL_MAXP = 128;
 // Loops of the planes (mus[i], nu), i < nplanes <= 3, sharing one axial-gauge
 // transformation; plane i's sums go to d_out[i * out_stride + k]; d_part holds
-// nblk * npairs * nplanes doubles.
+// nblk * npairs * nplanes doubles.  With st_loops, the loop kernels and the
+// reduction run there after an event (ev, recorded on st once U' is written):
+// only Omega and U' read the links, so st may go on to change them.
 cudaError_t launch_wilson_gf(int nc, int dtype, const void *links, const Geom &g, const int *mus, int nplanes,
                              int nu, const int *const *h_tab, int lmax, int tmax, int npairs, bool omega_ready,
                              void *scratch, double *d_part, int nblk, double *d_out, int out_stride,
-                             cudaStream_t st);
+                             cudaStream_t st, cudaStream_t st_loops = nullptr, cudaEvent_t ev = nullptr);
 
 int plaquette_blocks(const Geom &g);
 // ordered final reduction of nblk partials for each of n outputs

@@ -344,7 +344,9 @@ void klft_server::start_measure(Job &j, cudaEvent_t after) {
     }
     if (s == KLFT_OK && j.d.n_wilson > 0) {
       s = enqueue_wilson_spatial(lat, j.plan, false, d_out + kSlotWilson, KLFT_JOB_MAX_WILSON);
-      launches += 2 * (j.d.ndims - 1) + 2;  // omega, U' per plane, the loop kernel, a reduction per plane
+      // omega, U' per plane, the loop kernel, the reductions (one launch when the
+      // planes' sums are contiguous, i.e. the pair list fills its slots)
+      launches += (j.d.ndims - 1) + 2 + (j.d.n_wilson == KLFT_JOB_MAX_WILSON ? 1 : j.d.ndims - 1);
     }
     if (s == KLFT_OK && j.d.kind == KLFT_JOB_HMC) {
       s = hmc_enqueue_summary(lat, j.d.ntraj, d_out + kSlotHmc);

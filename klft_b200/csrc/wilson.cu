@@ -797,7 +797,8 @@ int wilson_gf_blocks(const Geom &g) {
 template <int N, typename T>
 static cudaError_t wilson_gf_t(const void *links, const Geom &g, const int *const *h_tab, int lmax, int tmax,
                                int npairs, const int *mus, int nplanes, int nu, bool omega_ready, void *scratch,
-                               double *d_part, int nblk, int *grid_used, cudaStream_t st) {
+                               double *d_part, int nblk, int *grid_used, cudaStream_t st, cudaStream_t stl,
+                               cudaEvent_t ev) {
   auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
   if (nplanes < 1 || nplanes > WC_MAXPL) return cudaErrorInvalidValue;
   if (npairs > WL_MAXP || lmax > WL_MAXP || tmax > 32767) return cudaErrorInvalidValue;
@@ -817,6 +818,13 @@ static cudaError_t wilson_gf_t(const void *links, const Geom &g, const int *cons
     const CField<N, T> up{(cx<T> *)(up0 + i * up_bytes), c[i].ncols * c[i].rows};
     uprime_kernel<N, T><<<(unsigned)(nct * ((c[i].rows + UP_RB - 1) / UP_RB)), 32 * UP_RB, 0, st>>>(U, g, c[i], om,
                                                                                                  pol, up);
+  }
+  // the loop kernels read U' only: on stl (if given) after U' is complete
+  if (stl) {
+    cudaError_t e = cudaEventRecord(ev, st);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(stl, ev, 0);
+    if (e != cudaSuccess) return e;
+    st = stl;
   }
   const CField<N, T> up{(cx<T> *)up0, c[0].ncols * c[0].rows};
   if (wcorr_eligible(tmax, h_tab[1], h_tab[0][lmax + 1])) {
@@ -899,12 +907,13 @@ static cudaError_t wilson_gf_t(const void *links, const Geom &g, const int *cons
 cudaError_t launch_wilson_gf(int nc, int dtype, const void *links, const Geom &g, const int *mus, int nplanes,
                              int nu, const int *const *h_tab, int lmax, int tmax, int npairs, bool omega_ready,
                              void *scratch, double *d_part, int nblk, double *d_out, int out_stride,
-                             cudaStream_t st) {
+                             cudaStream_t st, cudaStream_t st_loops, cudaEvent_t ev) {
   cudaError_t e = cudaErrorInvalidValue;
+  if (st_loops && !ev) return e;
   int grid = nblk;  // CTAs that wrote partial sums
 #define KLFT_WGF(NV, TV)                                                                                        \
   e = wilson_gf_t<NV, TV>(links, g, h_tab, lmax, tmax, npairs, mus, nplanes, nu, omega_ready, scratch, d_part, \
-                          nblk, &grid, st)
+                          nblk, &grid, st, st_loops, ev)
   if (dtype == 0) {
     if (nc == 1) KLFT_WGF(1, double);
     else if (nc == 2) KLFT_WGF(2, double);
@@ -916,6 +925,9 @@ cudaError_t launch_wilson_gf(int nc, int dtype, const void *links, const Geom &g
   }
 #undef KLFT_WGF
   if (e != cudaSuccess) return e;
+  if (st_loops) st = st_loops;
+  // plane i's sums at d_out + i * out_stride: one reduction launch when they are contiguous
+  if (out_stride == npairs) return launch_reduce_partials(d_part, grid, nplanes * npairs, d_out, st);
   for (int i = 0; i < nplanes && e == cudaSuccess; ++i)
     e = launch_reduce_partials(d_part + (size_t)i * npairs * grid, grid, npairs, d_out + (size_t)i * out_stride, st);
   return e;
