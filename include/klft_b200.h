@@ -4,7 +4,8 @@
  * Conventions
  *  - Every entry point returns klft_status; on failure klft_last_error() gives a
  *    thread-local message.  No exception crosses the ABI.
- *  - Opaque handles own device memory and one CUDA stream each.  Calls on one
+ *  - Opaque handles own device memory and one CUDA stream each (a lattice
+ *    used by klft_run_cycles gains a second one on that call).  Calls on one
  *    handle are serialised by the library; distinct handles may be used from
  *    different threads.  Calls return after their device work has completed.
  *  - Host link buffers use the interchange layout
@@ -106,8 +107,12 @@ klft_status klft_reunitarize(klft_lattice *lat);
 /* ncycles update-and-measure cycles enqueued back to back on the handle's stream,
  * as run_metropolis does them (Metropolis.hpp:204-218): one sweep, then (when
  * asked) GaugePlaquette and WilsonLoop_temporal over npairs (L, T) pairs.
- * acc_out[c], plaq_out[c], w_out[c*npairs + k] receive the results (each may be
- * NULL); device_ms the CUDA-event time of the whole sequence. */
+ * With loops to measure, the plaquette and the loop kernels run on a second
+ * stream of the handle (created on the first such call) beside the loops'
+ * gauge transformation and the next sweep, ordered by events; the results are
+ * those of the cycle order.  acc_out[c], plaq_out[c], w_out[c*npairs + k]
+ * receive the results (each may be NULL); device_ms the CUDA-event time of the
+ * whole sequence. */
 klft_status klft_run_cycles(klft_lattice *lat, double beta, double delta, int nhits, int proposal, double eps,
                             int ncycles, int measure_plaquette, const int *temporal_pairs, int npairs,
                             double *acc_out, double *plaq_out, double *w_out, double *device_ms);
