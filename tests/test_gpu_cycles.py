@@ -32,6 +32,22 @@ def test_cycles_match_single_calls(L, nc, pairs, precision, rtol, atol):
     np.testing.assert_array_equal(a.download(), b.download())
 
 
+@pytest.mark.parametrize("precision,rtol,atol", [("fp64", 1e-12, 1e-14), ("mixed", 0.0, 2e-6)])
+def test_cycles_loops_without_plaquette_match_single_calls(precision, rtol, atol):
+    """Loops measured and the plaquette not: the loop kernels of each cycle run
+    beside the next cycle's sweep with nothing else on the second stream."""
+    pairs = [(l, t) for l in range(1, 5) for t in range(1, 9)]
+    a = GaugeField([4, 6, 4, 8], 3, precision, "hot", 77)
+    b = GaugeField([4, 6, 4, 8], 3, precision, "hot", 77)
+    a.set_stream(77, 2)
+    b.set_stream(77, 2)
+    acc, _, w, _ = a.run_cycles(6.0, 0.0, 4, 4, "exp", 0.3, False, pairs)
+    for c in range(4):
+        assert acc[c] == b.metropolis(6.0, 0.0, 4, 1, "exp", 0.3)[0]
+        np.testing.assert_allclose(w[c], b.wilson_loop_temporal(pairs), rtol=rtol, atol=atol)
+    np.testing.assert_array_equal(a.download(), b.download())
+
+
 @pytest.mark.parametrize("L,nc,precision", [([8, 8, 8, 8], 1, "fp64"), ([4, 4, 6, 4], 3, "mixed"),
                                             ([6, 4, 8], 2, "fp64"), ([8, 6], 3, "fp64")])
 def test_run_metropolis_fused_matches_single_calls(L, nc, precision):
