@@ -74,7 +74,7 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::v)
     bool ok = false;
     const Site x = link_pass_site(c.g, t, val & 1, ND, ok);
     if (ok && t < link_pass_threads(c.g, ND))
-      nacc = link_update_exp<ND, T, DF, MU>(U, c.g, x, MU >= 0 ? MU : val >> 1, c.a, *c.ctr, c.df);
+      nacc = link_update_exp<ND, T, DF, MU>(U, c.g, x, MU, c.a, *c.ctr, c.df);
   } else {
     if (t < c.g.Vh) nacc = site_update_ref<NC, ND, T, DF>(U, c.g, pass_site(c.g, t, val, ND), c.a, *c.ctr, c.df);
   }

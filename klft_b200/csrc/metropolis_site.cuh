@@ -220,11 +220,13 @@ KLFT_D void exp_hit(const Mat<3, T> &X, bool first, const Mat<3, T> &M0, T bnc, 
 }
 
 // The hits of link U_mu(x) (hit h = mu * nHits + hit of the site's stream).
-// MU >= 0: the pass's direction at compile time (mu == MU), for the staples
-// with compiled site steps; MU = -1 (batches) reads it at run time.
-template <int ND, typename T, bool DF, int MU = -1>
+// MU: the pass's direction at compile time (mu == MU; every link pass, single
+// lattice or batch, is one kernel instance per direction), for the staples
+// with compiled site steps.
+template <int ND, typename T, bool DF, int MU>
 KLFT_D int link_update_exp(const Links<3, T> &U, const Geom &g, const Site &x, int mu, const MetroArgs &a,
                            uint32_t sweep, const Defect &df) {
+  static_assert(MU >= 0 && MU < ND, "link passes are compiled per direction");
   if (open_link(g, x, mu)) return 0;
   int nacc = 0;
   const ExpHitStream hs{(uint32_t)a.seed, (uint32_t)(a.seed >> 32) ^ (uint32_t)a.chain, site_lex(g, x), sweep, a.bm};
@@ -236,11 +238,8 @@ KLFT_D int link_update_exp(const Links<3, T> &U, const Geom &g, const Site &x, i
   // M0 = U0 S stays fixed; A is the product of the accepted X, so the current
   // link is A U0 and Re Tr(X A U0 S) = Re Tr((X A) M0): one product X A per hit
   Mat<3, T> S;
-  constexpr int MC = MU >= 0 ? MU : 0;
-  if constexpr (MU >= 0 && !DF && sizeof(T) == 4) S = staple_su3_2row_ct<ND, MC>(U, g, x);
-  else if constexpr (MU >= 0) S = staple_ct<3, ND, MC, T, DF>(U, g, x, df);
-  else if constexpr (sizeof(T) == 4 && !DF) S = staple_su3_2row<ND>(U, g, x, mu);
-  else S = staple<3, ND, T, DF>(U, g, x, mu, df);
+  if constexpr (!DF && sizeof(T) == 4) S = staple_su3_2row_ct<ND, MU>(U, g, x);
+  else S = staple_ct<3, ND, MU, T, DF>(U, g, x, df);
   const Mat<3, T> M0 = mul(U.load(lx, mu), S);
   Mat<3, T> A = mident<3, T>();
   T trO = retr_diag(M0);

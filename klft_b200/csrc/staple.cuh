@@ -79,40 +79,10 @@ template <typename T> KLFT_D void mul_dn_rows01(const Mat<3, T> &a, const Mat<3,
       c.e[i][j] = conj(a.e[0][i]) * b.e[0][j] + conj(a.e[1][i]) * b.e[1][j] + conj(a.e[2][i]) * b.e[2][j];
 }
 
-template <int ND>
-KLFT_D Mat<3, float> staple_su3_2row(const Links<3, float> &U, const Geom &g, const Site &x, int mu) {
-  Mat<3, float> S = mzero<3, float>();
-  const Site xpmu = site_up(g, x, mu);
-#pragma unroll 1
-  for (int nu = 0; nu < ND; ++nu) {
-    if (nu == mu) continue;
-    const Site xpnu = site_up(g, x, nu);
-    Mat<3, float> cb, f;
-    mul_rows01(U.load_rows01(site_lin(g, x), nu), U.load(site_lin(g, xpnu), mu), cb);
-    complete_row2(cb);
-    mul_nd_rows01(U.load_rows01(site_lin(g, xpmu), nu), cb, f);
-    complete_row2(f);
-    madd(S, f);
-  }
-#pragma unroll 1
-  for (int nu = 0; nu < ND; ++nu) {
-    if (nu == mu) continue;
-    const Site xpmu_mnu = site_dn(g, xpmu, nu);
-    const Site xmnu = site_dn(g, x, nu);
-    Mat<3, float> ed, f;
-    mul_rows01(U.load_rows01(site_lin(g, xmnu), mu), U.load(site_lin(g, xpmu_mnu), nu), ed);
-    complete_row2(ed);
-    mul_dn_rows01(ed, U.load(site_lin(g, xmnu), nu), f);
-    complete_row2(f);
-    madd(S, f);
-  }
-  return S;
-}
-
-// staple_su3_2row with mu fixed at compile time and the nu loops unrolled (the
-// same products in the same order): each link pass compiles its own site
-// steps and can issue the loads of several terms ahead of their products.
-// 1.62 -> 1.50 ms per SU(3) 32^4 sweep (1.56 with the nu loops rolled).
+// The two-row staple with mu fixed at compile time and the nu loops unrolled:
+// each link pass compiles its own site steps and can issue the loads of
+// several terms ahead of their products.  1.62 -> 1.50 ms per SU(3) 32^4 sweep
+// against a run-time mu (1.56 with the nu loops rolled).
 template <int ND, int MU>
 KLFT_D Mat<3, float> staple_su3_2row_ct(const Links<3, float> &U, const Geom &g, const Site &x) {
   Mat<3, float> S = mzero<3, float>();
