@@ -5,7 +5,8 @@
  *  - Every entry point returns klft_status; on failure klft_last_error() gives a
  *    thread-local message.  No exception crosses the ABI.
  *  - Opaque handles own device memory and one CUDA stream each (a lattice
- *    used by klft_run_cycles gains a second one on that call).  Calls on one
+ *    measured by klft_run_cycles or klft_run_metropolis gains a second one on
+ *    that call).  Calls on one
  *    handle are serialised by the library; distinct handles may be used from
  *    different threads.  Calls return after their device work has completed.
  *  - Host link buffers use the interchange layout

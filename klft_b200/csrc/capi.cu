@@ -633,9 +633,13 @@ klft_status klft_run_metropolis(klft_lattice *lat, double beta, double delta, in
   const int npw = nplanar > 0 && nmeas > 0 ? nplanes * nplanar : 0;
   const size_t per = 1 + (size_t)ntw + (size_t)npw;
   CK(lat->s_aux.ensure((size_t)nsweeps * sizeof(unsigned long long)));
-  CK(lat->s_wl.ensure(((size_t)nmeas * per + 1) * sizeof(double)));
+  // wl: the measurements' results, then the plaquette's block partials (apart
+  // from the loop kernels', which may run at the same time)
+  const int nblk_plaq = plaquette_blocks(lat->g);
+  CK(lat->s_wl.ensure(((size_t)nmeas * per + 1 + (size_t)nblk_plaq) * sizeof(double)));
   unsigned long long *d_nacc = (unsigned long long *)lat->s_aux.ptr;
   double *d_res = (double *)lat->s_wl.ptr;
+  double *d_plaq_part = d_res + (size_t)nmeas * per + 1;
   // plans: temporal loops along nu = Nd-1, one plan per distinct nu of the planar list
   CK(lat->s_tab.ensure((2 * (size_t)ntemporal + (size_t)nplanes * 2 * nplanar) * sizeof(int) + 16));
   WilsonPlan tplan;
@@ -651,10 +655,21 @@ klft_status klft_run_metropolis(klft_lattice *lat, double beta, double delta, in
     if (s != KLFT_OK) return s;
     toff += 2 * (size_t)nplanar;
   }
-  {
-    const int nblk = plaquette_blocks(lat->g);
-    if (lat->s_part.cap < (size_t)nblk * sizeof(double)) CK(lat->s_part.ensure((size_t)nblk * sizeof(double)));
+  // As in klft_run_cycles: the plaquette on the handle's second stream beside
+  // the loops' axial-gauge transformation, and (with no planar loops, which
+  // would share the loop scratch) the temporal loop kernel beside the sweeps
+  // that follow; events order the rest.
+  const bool fork = do_plaq && (ntw > 0 || npw > 0);
+  const bool loops_side = ntw > 0 && tplan.gf && npw == 0;
+  if ((fork || loops_side) && !lat->side) {
+    CK(cudaStreamCreateWithFlags(&lat->side, cudaStreamNonBlocking));
+    for (cudaEvent_t *ev : {&lat->ev_fork, &lat->ev_join, &lat->ev_up, &lat->ev_loops})
+      CK(cudaEventCreateWithFlags(ev, cudaEventDisableTiming));
   }
+  auto join_side = [&] {
+    if ((fork || loops_side) && cudaEventRecord(lat->ev_join, lat->side) == cudaSuccess)
+      cudaStreamWaitEvent(lat->stream, lat->ev_join, 0);
+  };
   CK(cudaMemsetAsync(d_nacc, 0, (size_t)nsweeps * sizeof(unsigned long long), lat->stream));
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
@@ -663,26 +678,46 @@ klft_status klft_run_metropolis(klft_lattice *lat, double beta, double delta, in
   int m = 0;
   for (int step = 0; step < nsweeps; ++step) {
     klft_status s = enqueue_sweeps(lat, beta, delta, nhits, proposal, eps, 1, d_nacc + step, lat->defect);
-    if (s != KLFT_OK) return s;
+    if (s != KLFT_OK) {
+      join_side();
+      return s;
+    }
     if (!(interval > 0 && step % interval == 0 && step != 0)) continue;
     double *slot = d_res + (size_t)m * per;
-    if (do_plaq)
-      CK(launch_plaquette(lat->nc, lat->dtype(), lat->links, lat->g, (double *)lat->s_part.ptr,
-                          plaquette_blocks(lat->g), slot, lat->stream));
+    cudaError_t e = cudaSuccess;
+    if (fork) {
+      e = cudaEventRecord(lat->ev_fork, lat->stream);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(lat->side, lat->ev_fork, 0);
+    }
+    if (e == cudaSuccess && do_plaq)
+      e = launch_plaquette(lat->nc, lat->dtype(), lat->links, lat->g, d_plaq_part, nblk_plaq, slot,
+                           fork ? lat->side : lat->stream);
+    if (e == cudaSuccess && fork) e = cudaEventRecord(lat->ev_join, lat->side);
     int last_nu = -1;
-    if (ntw > 0) {
-      s = enqueue_wilson_spatial(lat, tplan, false, slot + 1, ntemporal);
-      if (s != KLFT_OK) return s;
+    if (e == cudaSuccess && ntw > 0) {
+      // U' of this measurement after the loops of the previous one
+      if (loops_side && m > 0) e = cudaStreamWaitEvent(lat->stream, lat->ev_loops, 0);
+      if (e == cudaSuccess)
+        s = enqueue_wilson_spatial(lat, tplan, false, slot + 1, ntemporal, loops_side ? lat->side : nullptr,
+                                   lat->ev_up);
+      if (e == cudaSuccess && s == KLFT_OK && loops_side) e = cudaEventRecord(lat->ev_loops, lat->side);
       last_nu = nd - 1;
     }
-    for (int q = 0; q < (int)pplan.size(); ++q) {
+    for (int q = 0; q < (int)pplan.size() && s == KLFT_OK && e == cudaSuccess; ++q) {
       const int mu = planes[2 * q], nu = planes[2 * q + 1];
       s = enqueue_wilson_plane(lat, pplan[q], mu, nu, last_nu == nu, slot + 1 + ntw + (size_t)q * nplanar);
-      if (s != KLFT_OK) return s;
       last_nu = nu;
+    }
+    // the next sweep after the plaquette
+    if (s == KLFT_OK && e == cudaSuccess && fork) e = cudaStreamWaitEvent(lat->stream, lat->ev_join, 0);
+    if (s != KLFT_OK || e != cudaSuccess) {
+      join_side();
+      return s != KLFT_OK ? s : cuda_fail(e, "klft_run_metropolis");
     }
     ++m;
   }
+  // the result copy after the last loops
+  if (loops_side) CK(cudaStreamWaitEvent(lat->stream, lat->ev_loops, 0));
   CK(cudaEventRecord(e1, lat->stream));
   std::vector<unsigned long long> h_nacc(nsweeps);
   std::vector<double> h_res((size_t)nmeas * per);

@@ -50,7 +50,9 @@ def test_cycles_loops_without_plaquette_match_single_calls(precision, rtol, atol
 
 @pytest.mark.parametrize("L,nc,precision", [([8, 8, 8, 8], 1, "fp64"), ([4, 4, 6, 4], 3, "mixed"),
                                             ([6, 4, 8], 2, "fp64"), ([8, 6], 3, "fp64")])
-def test_run_metropolis_fused_matches_single_calls(L, nc, precision):
+# without planar loops the temporal loop kernel runs beside the following sweeps
+@pytest.mark.parametrize("planar", [True, False])
+def test_run_metropolis_fused_matches_single_calls(L, nc, precision, planar):
     """klft_run_metropolis (measurements every `interval` sweeps, step 0
     excluded, temporal and planar loops, all enqueued) against the same run
     through the single-call API, measurement by measurement, bit for bit."""
@@ -58,8 +60,8 @@ def test_run_metropolis_fused_matches_single_calls(L, nc, precision):
     prop = "exp" if nc == 3 else "reference"
     nd = len(L)
     tp = [(1, 1), (2, 2), (2, 1)]
-    planes = [(0, 1), (1, 0)] + ([(1, 2), (2, 0)] if nd > 2 else [])
-    pp = [(1, 1), (2, 2), (2, 1)]
+    planes = ([(0, 1), (1, 0)] + ([(1, 2), (2, 0)] if nd > 2 else [])) if planar else []
+    pp = [(1, 1), (2, 2), (2, 1)] if planar else []
     a = GaugeField(L, nc, precision, "hot", 32091)
     b = GaugeField(L, nc, precision, "hot", 32091)
     a.set_stream(32091, 1)
