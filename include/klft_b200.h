@@ -6,9 +6,9 @@
  *    thread-local message.  No exception crosses the ABI.
  *  - Opaque handles own device memory and one CUDA stream each (a lattice
  *    measured by klft_run_cycles or klft_run_metropolis gains a second one on
- *    that call).  Calls on one
- *    handle are serialised by the library; distinct handles may be used from
- *    different threads.  Calls return after their device work has completed.
+ *    that call).  Calls on one handle are serialised by the library; distinct
+ *    handles may be used from different threads.  Calls return after their
+ *    device work has completed.
  *  - Host link buffers use the interchange layout
  *        U[(((site*Nd + mu)*Nc + i)*Nc + j)*2 + {0: re, 1: im}]   (double)
  *    with site = x0 + L0*(x1 + L1*(x2 + L2*x3)).
